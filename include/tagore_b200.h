@@ -1,0 +1,167 @@
+/* tagore_b200.h -- C ABI of the B200 graph-index builder.
+ *
+ * Drop-in boundary for the Python module `Tagore` of ZJU-DAILY/Tagore
+ * (pybind.cu:393-398). Every function returns a status code; on failure
+ * tagore_last_error() gives a one-line message (thread-local). No function
+ * exits the process. Device buffers are plain pointers on the current device.
+ */
+#ifndef TAGORE_B200_H
+#define TAGORE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  TAGORE_OK = 0,
+  TAGORE_EINVAL = 1,   /* bad argument or unsupported combination */
+  TAGORE_EIO = 2,      /* file missing, truncated or unwritable */
+  TAGORE_ENOMEM = 3,   /* host or device allocation failed */
+  TAGORE_ECUDA = 4,    /* a CUDA call failed */
+  TAGORE_ETIMEOUT = 5  /* a bounded wait ran out */
+};
+
+enum { TAGORE_KNN_CHOSEN = 0, TAGORE_KNN_PLAIN = 1 };
+
+/* The reference's eight device buffers in its capsule order
+ * (pybind.cu:132-141), plus project buffers. Ownership: created by
+ * tagore_gnn_descent / tagore_state_alloc, released by tagore_state_free. */
+typedef struct TagoreKnnState {
+  uint32_t n, dim, k;
+  int32_t device;
+  float norm_factor;        /* power of ten applied to the base (pybind.cu:24-36) */
+  uint32_t ep;              /* entry point of the last NSG/Vamana prune */
+  void* graph;              /* [0] u32 [n*k]: kNN ids sorted by distance; pruned rows after Pruning */
+  void* reverse_graph;      /* [1] u32 [n*128] */
+  void* data;               /* [2] f16 [n*dim], scaled by norm_factor */
+  void* nei_distance;       /* [3] f32 [n*k] */
+  void* reverse_distance;   /* [4] f32 [n*128] */
+  void* reverse_num;        /* [5] u32 [n] */
+  void* center;             /* [6] f16 [dim], scaled */
+  void* hybrid_list;        /* [7] u32 [n*128] */
+  void* norms;              /* f32 [n]: exact squared norms of the FP16 base */
+  uint32_t owns;            /* 1 when tagore_state_free releases the buffers */
+  uint32_t pad_;
+} TagoreKnnState;
+
+typedef struct TagoreKnnParams {
+  uint32_t k;        /* degree of the kNN graph (K) */
+  uint32_t n;        /* POINTS; the fvecs loader takes the count from the file */
+  uint32_t dim;      /* DIM */
+  uint32_t iters;    /* iterations; the reference runs iters/2 + iters/2 */
+  uint32_t mode;     /* TAGORE_KNN_CHOSEN or TAGORE_KNN_PLAIN */
+  uint32_t sample;   /* forward samples per list and iteration (0: 32) */
+  uint32_t per_row;  /* proposals kept per local-join row (0: default) */
+  uint32_t rescale;  /* 1: power-of-ten rescale as GNN_descent; 0: none (largeIndex) */
+  uint64_t seed;
+} TagoreKnnParams;
+
+typedef struct TagorePruneParams {
+  uint32_t k, n, dim;
+  uint32_t final_degree; /* FINAL_DEGREE */
+  uint32_t topm;         /* TOPM (m), default 64 */
+  float thre;            /* threshold: alpha for Vamana, cos(angle) for NSSG */
+} TagorePruneParams;
+
+typedef struct TagoreLargeParams {
+  uint32_t dim, k, cluster_num, max_points;
+  const char* data_prefix;        /* cluster files data_prefix + cid: [u32 n][n*dim f32] */
+  const char* local_prefix;       /* spill files of evicted local graphs */
+  const char* index_store_path;   /* final DiskANN-style index */
+  uint32_t max_degree, buffer_size;
+  uint32_t num;                   /* total points */
+  const char* centers_path;       /* num x (u32 first, u32 second) cluster ids */
+  float thre;
+  uint32_t final_degree, topm;
+  uint32_t knn_iters;             /* GNN-Descent iterations per cluster (reference: 8 + 8) */
+  uint32_t mode;                  /* TAGORE_KNN_CHOSEN or TAGORE_KNN_PLAIN */
+} TagoreLargeParams;
+
+/* Tagore.GNN_descent(K, POINTS, DIM, iter, fname) (pybind.cu:19-142):
+ * loads an fvecs file and builds the kNN graph on the current device. */
+int tagore_gnn_descent(const TagoreKnnParams* p, const char* fvecs_path, TagoreKnnState* out);
+
+/* Same as tagore_gnn_descent with the FP32 base in host memory
+ * (n x dim, row-major) instead of a file. */
+int tagore_gnn_descent_host(const TagoreKnnParams* p, const float* data, uint32_t n, uint32_t dim,
+                            TagoreKnnState* out);
+
+/* Tagore.Pruning(K, POINTS, DIM, FINAL_DEGREE, TOPM, ptrs, index_type, thre,
+ * index_path) (pybind.cu:145-229): prunes in place and writes the index file
+ * (NSG, Vamana, NSSG, CAGRA or DPG layout, src/common.cu:151-248). An empty or
+ * NULL index_path skips the file. */
+int tagore_pruning(const TagorePruneParams* p, TagoreKnnState* st, const char* index_type,
+                   const char* index_path);
+
+/* Tagore.Pruning_with_CFS(K, POINTS, DIM, FINAL_DEGREE, TOPM, ptrs, mode,
+ * metric, thre) (pybind.cu:232-295): Collect ('path', '2-hop', '1-hop'),
+ * Filter+Store ('dist', 'angle', 'rank'); the result stays in st->graph. */
+int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const char* mode,
+                       const char* metric);
+
+/* Tagore.largeIndex(devicelist, DIM, K, cluster_num, max_points, ...)
+ * (pybind.cu:298-391) for a single device (devicelist = [0]). */
+int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev);
+
+/* cal_ep_gpu (src/Tagore_src.cu:1889-2058) alone: entry point of the graph
+ * held in st (kNN rows) toward st->center. */
+int tagore_entry_point(TagoreKnnState* st, uint32_t topm, uint32_t* ep);
+
+/* Allocates the eight buffers (and norms) for n x dim with degree k on the
+ * current device, zero-filled; reverse_num starts at 0 as after GNN_descent. */
+int tagore_state_alloc(uint32_t n, uint32_t dim, uint32_t k, TagoreKnnState* out);
+
+/* Releases buffers owned by the state (the capsule destructors of pybind.cu:133-140). */
+int tagore_state_free(TagoreKnnState* st);
+
+/* Copies between a host array and one of the state's buffers, by capsule
+ * index 0..7 (8 = norms); bytes must not exceed the buffer. */
+int tagore_state_upload(TagoreKnnState* st, int which, const void* host, size_t bytes);
+int tagore_state_download(const TagoreKnnState* st, int which, void* host, size_t bytes);
+
+/* Byte size of buffer `which` of the state. */
+size_t tagore_state_bytes(const TagoreKnnState* st, int which);
+
+/* One whole build from host memory to host memory: rescale + FP16 base,
+ * kNN graph (p), CFS 'path'/'dist' prune with final_degree/topm/thre, and the
+ * pruned rows copied back as [deg, ids...] stride-k rows into out_graph
+ * (n*k u32). *ep_out gets the entry point. Used for the end-to-end timing. */
+int tagore_build_index_host(const TagoreKnnParams* p, const float* data, uint32_t n, uint32_t dim,
+                            uint32_t final_degree, uint32_t topm, float thre, uint32_t* out_graph,
+                            uint32_t* ep_out);
+
+/* Index writers (src/common.cu:151-248), from host rows. */
+int tagore_store_nsg(const char* path, const uint32_t* graph, uint32_t width, uint32_t ep,
+                     uint32_t n, uint32_t k);
+int tagore_store_vamana(const char* path, const uint32_t* graph, uint32_t ep, uint32_t n,
+                        uint32_t k);
+int tagore_store_nssg(const char* path, const uint32_t* graph, uint32_t width, uint32_t n,
+                      uint32_t k);
+int tagore_store_dpg(const char* path, const uint32_t* graph, uint32_t n, uint32_t degree);
+int tagore_store_cagra(const char* path, const uint32_t* graph, uint32_t n, uint32_t degree);
+
+/* fvecs loader (src/common.cu:6-22): count from the file size, dims from the
+ * first record. tagore_load_fvecs_header reports n and dim only. */
+int tagore_load_fvecs_header(const char* path, uint32_t* n, uint32_t* dim);
+int tagore_load_fvecs(const char* path, float* out, uint32_t n, uint32_t dim);
+
+/* Timings of the last build on this thread (milliseconds). */
+typedef struct TagoreTimings {
+  double knn_ms, prune_ms, prep_ms, total_ms;
+  uint64_t kernel_launches;
+} TagoreTimings;
+int tagore_last_timings(TagoreTimings* t);
+
+/* Frees a device buffer this library allocated (capsule destructor). */
+int tagore_device_free(void* p);
+
+const char* tagore_last_error(void);
+const char* tagore_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TAGORE_B200_H */

@@ -1,0 +1,31 @@
+#!/bin/sh
+# Compiles the reference Tagore module from its own four .cu files, read in
+# place, for sm_100a into oracle/_ref/ (git-ignored). The result is used only
+# to generate golden fixtures (tests/golden/make_golden.py) on a GPU host.
+# The reference includes <boost/dynamic_bitset.hpp> for dead CPU code only
+# (src/common.cu:65-148); a small stand-in header is written instead.
+set -e
+REF=${TAGORE_REF:-/root/reference}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+mkdir -p "$OUT/include/boost"
+cat > "$OUT/include/boost/dynamic_bitset.hpp" <<'HDR'
+#pragma once
+#include <cstddef>
+#include <vector>
+namespace boost {
+template <class Block = unsigned long>
+struct dynamic_bitset : std::vector<bool> {
+  dynamic_bitset(std::size_t n, unsigned long v) : std::vector<bool>(n, v != 0) {}
+};
+}
+HDR
+PYINC=$(python3 -c 'import sysconfig; print(sysconfig.get_paths()["include"])')
+PBINC=$(python3 -c 'import pybind11; print(pybind11.get_include())')
+SUFFIX=$(python3 -c 'import sysconfig; print(sysconfig.get_config_var("EXT_SUFFIX"))')
+/usr/local/cuda/bin/nvcc -ccbin /usr/bin/g++ -gencode arch=compute_100a,code=sm_100a -rdc=true -O3 \
+  -std=c++17 -Xcompiler -fPIC,-fopenmp -w \
+  -I"$REF/include" -I"$OUT/include" -I"$PBINC" -I"$PYINC" -shared \
+  "$REF/pybind.cu" "$REF/src/common.cu" "$REF/src/Tagore_src.cu" "$REF/src/large_index.cu" \
+  -o "$OUT/Tagore$SUFFIX" -lgomp
+echo "built $OUT/Tagore$SUFFIX"

@@ -1,0 +1,323 @@
+// capi.cu -- the C ABI (include/tagore_b200.h): argument checks, buffer
+// ownership, streams, timings and error reporting around the kernel files.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "internal.h"
+
+namespace tagore {
+
+static thread_local std::string g_err;
+static thread_local TagoreTimings g_times{};
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+  const char* base = std::strrchr(file, '/');
+  fail(e == cudaErrorMemoryAllocation ? TAGORE_ENOMEM : TAGORE_ECUDA, "%s failed: %s (%s:%d)", what,
+       cudaGetErrorString(e), base ? base + 1 : file, line);
+  return e == cudaErrorMemoryAllocation ? TAGORE_ENOMEM : TAGORE_ECUDA;
+}
+
+namespace {
+
+// A non-blocking stream owned by one API call.
+struct Stream {
+  cudaStream_t s = nullptr;
+  int init() {
+    TG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return TAGORE_OK;
+  }
+  ~Stream() {
+    if (s) cudaStreamDestroy(s);
+  }
+};
+
+struct Timer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  Timer() {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+  }
+  ~Timer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  void start(cudaStream_t s) { cudaEventRecord(a, s); }
+  double stop(cudaStream_t s) {
+    cudaEventRecord(b, s);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+  }
+};
+
+size_t buffer_bytes(uint32_t n, uint32_t dim, uint32_t k, int which) {
+  switch (which) {
+    case 0: return (size_t)n * k * 4;
+    case 1: return (size_t)n * 128 * 4;
+    case 2: return (size_t)n * dim * 2;
+    case 3: return (size_t)n * k * 4;
+    case 4: return (size_t)n * 128 * 4;
+    case 5: return (size_t)n * 4;
+    case 6: return (size_t)dim * 2;
+    case 7: return (size_t)n * 128 * 4;
+    case 8: return (size_t)n * 4;
+    default: return 0;
+  }
+}
+
+void** slot(TagoreKnnState* st, int which) {
+  switch (which) {
+    case 0: return &st->graph;
+    case 1: return &st->reverse_graph;
+    case 2: return &st->data;
+    case 3: return &st->nei_distance;
+    case 4: return &st->reverse_distance;
+    case 5: return &st->reverse_num;
+    case 6: return &st->center;
+    case 7: return &st->hybrid_list;
+    case 8: return &st->norms;
+    default: return nullptr;
+  }
+}
+
+int check_state(const TagoreKnnState* st) {
+  if (!st || !st->graph || !st->data || !st->nei_distance || !st->reverse_graph ||
+      !st->reverse_distance || !st->reverse_num || !st->center || !st->hybrid_list)
+    return fail(TAGORE_EINVAL, "state has missing buffers");
+  return TAGORE_OK;
+}
+
+int check_prune(const TagorePruneParams* p, TagoreKnnState* st) {
+  if (!p) return fail(TAGORE_EINVAL, "null params");
+  TG_TRY(check_state(st));
+  if (p->k != st->k || p->n != st->n || p->dim != st->dim)
+    return fail(TAGORE_EINVAL, "K/POINTS/DIM (%u/%u/%u) differ from the graph's (%u/%u/%u)", p->k,
+                p->n, p->dim, st->k, st->n, st->dim);
+  return TAGORE_OK;
+}
+
+int build_from_device(const TagoreKnnParams* p, const float* raw_dev, const float* host_for_center,
+                      uint32_t n, uint32_t dim, TagoreKnnState* st, cudaStream_t s) {
+  const bool rescale = p->rescale != 0;
+  st->norm_factor = host_factor(host_for_center, dim, rescale);
+  Timer t0;
+  t0.start(s);
+  TG_TRY(prep_base(raw_dev, n, dim, st->norm_factor, (__half*)st->data, (float*)st->norms, s));
+  std::vector<uint16_t> center(dim);
+  std::thread cth(host_center, host_for_center, n, dim, st->norm_factor, center.data());
+  KnnArgs a{p->k, p->iters, p->mode, p->sample, p->per_row, p->seed};
+  KnnStats ks{};
+  const int rc = knn_build(dev_of(st), (const float*)st->norms, a, &ks, s);
+  g_times.knn_ms = t0.stop(s);
+  cth.join();
+  TG_TRY(rc);
+  TG_CUDA(cudaMemcpyAsync(st->center, center.data(), (size_t)dim * 2, cudaMemcpyHostToDevice, s));
+  TG_CUDA(cudaStreamSynchronize(s));
+  return TAGORE_OK;
+}
+
+}  // namespace
+}  // namespace tagore
+
+using namespace tagore;
+
+extern "C" {
+
+const char* tagore_last_error(void) { return g_err.c_str(); }
+const char* tagore_version(void) { return "tagore_b200 0.1 (sm_100a)"; }
+
+int tagore_last_timings(TagoreTimings* t) {
+  if (!t) return fail(TAGORE_EINVAL, "null timings");
+  *t = g_times;
+  return TAGORE_OK;
+}
+
+size_t tagore_state_bytes(const TagoreKnnState* st, int which) {
+  return st ? buffer_bytes(st->n, st->dim, st->k, which) : 0;
+}
+
+int tagore_state_alloc(uint32_t n, uint32_t dim, uint32_t k, TagoreKnnState* out) {
+  if (!out) return fail(TAGORE_EINVAL, "null state");
+  if (n == 0 || dim == 0 || k == 0) return fail(TAGORE_EINVAL, "n, dim and k must be positive");
+  std::memset(out, 0, sizeof(*out));
+  out->n = n;
+  out->dim = dim;
+  out->k = k;
+  out->norm_factor = 1.0f;
+  out->owns = 1;
+  cudaGetDevice(&out->device);
+  for (int w = 0; w <= 8; ++w) {
+    void** p = slot(out, w);
+    const size_t b = buffer_bytes(n, dim, k, w);
+    cudaError_t e = cudaMalloc(p, b);
+    if (e == cudaSuccess) e = cudaMemset(*p, 0, b);
+    if (e != cudaSuccess) {
+      tagore_state_free(out);
+      return cuda_fail(e, "cudaMalloc(state)", __FILE__, __LINE__);
+    }
+  }
+  return TAGORE_OK;
+}
+
+int tagore_device_free(void* p) {
+  if (p) TG_CUDA(cudaFree(p));
+  return TAGORE_OK;
+}
+
+int tagore_state_free(TagoreKnnState* st) {
+  if (!st) return TAGORE_OK;
+  if (st->owns) {
+    for (int w = 0; w <= 8; ++w) {
+      void** p = slot(st, w);
+      if (*p) cudaFree(*p);
+      *p = nullptr;
+    }
+  }
+  st->owns = 0;
+  return TAGORE_OK;
+}
+
+int tagore_state_upload(TagoreKnnState* st, int which, const void* host, size_t bytes) {
+  if (!st || !host || which < 0 || which > 8 || !*slot(st, which))
+    return fail(TAGORE_EINVAL, "bad upload arguments");
+  if (bytes > buffer_bytes(st->n, st->dim, st->k, which))
+    return fail(TAGORE_EINVAL, "upload of %zu bytes exceeds buffer %d", bytes, which);
+  TG_CUDA(cudaMemcpy(*slot(st, which), host, bytes, cudaMemcpyHostToDevice));
+  return TAGORE_OK;
+}
+
+int tagore_state_download(const TagoreKnnState* st, int which, void* host, size_t bytes) {
+  if (!st || !host || which < 0 || which > 8)
+    return fail(TAGORE_EINVAL, "bad download arguments");
+  void* p = *slot(const_cast<TagoreKnnState*>(st), which);
+  if (!p) return fail(TAGORE_EINVAL, "buffer %d is not allocated", which);
+  if (bytes > buffer_bytes(st->n, st->dim, st->k, which))
+    return fail(TAGORE_EINVAL, "download of %zu bytes exceeds buffer %d", bytes, which);
+  TG_CUDA(cudaMemcpy(host, p, bytes, cudaMemcpyDeviceToHost));
+  return TAGORE_OK;
+}
+
+int tagore_gnn_descent_host(const TagoreKnnParams* p, const float* data, uint32_t n, uint32_t dim,
+                            TagoreKnnState* out) {
+  if (!p || !data || !out) return fail(TAGORE_EINVAL, "null argument");
+  if (dim != p->dim) return fail(TAGORE_EINVAL, "DIM %u differs from the data's %u", p->dim, dim);
+  if (dim % 4) return fail(TAGORE_EINVAL, "DIM must be a multiple of 4 (got %u)", dim);
+  if (p->k == 0 || p->k >= n) return fail(TAGORE_EINVAL, "need POINTS > K >= 1");
+  Stream st;
+  TG_TRY(st.init());
+  TG_TRY(tagore_state_alloc(n, dim, p->k, out));
+  float* raw = nullptr;
+  cudaError_t e = cudaMallocAsync((void**)&raw, (size_t)n * dim * 4, st.s);
+  if (e != cudaSuccess) {
+    tagore_state_free(out);
+    return cuda_fail(e, "cudaMallocAsync(raw)", __FILE__, __LINE__);
+  }
+  int rc = TAGORE_OK;
+  e = cudaMemcpyAsync(raw, data, (size_t)n * dim * 4, cudaMemcpyHostToDevice, st.s);
+  if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(raw)", __FILE__, __LINE__);
+  if (rc == TAGORE_OK) rc = build_from_device(p, raw, data, n, dim, out, st.s);
+  cudaFreeAsync(raw, st.s);
+  cudaStreamSynchronize(st.s);
+  if (rc != TAGORE_OK) tagore_state_free(out);
+  return rc;
+}
+
+int tagore_gnn_descent(const TagoreKnnParams* p, const char* fvecs_path, TagoreKnnState* out) {
+  if (!p || !fvecs_path || !out) return fail(TAGORE_EINVAL, "null argument");
+  uint32_t n = 0, dim = 0;
+  TG_TRY(tagore_load_fvecs_header(fvecs_path, &n, &dim));
+  if (dim != p->dim) return fail(TAGORE_EINVAL, "file DIM %u differs from DIM %u", dim, p->dim);
+  std::vector<float> host((size_t)n * dim);
+  TG_TRY(tagore_load_fvecs(fvecs_path, host.data(), n, dim));
+  return tagore_gnn_descent_host(p, host.data(), n, dim, out);
+}
+
+int tagore_entry_point(TagoreKnnState* st, uint32_t topm, uint32_t* ep) {
+  TG_TRY(check_state(st));
+  if (!ep || topm == 0) return fail(TAGORE_EINVAL, "bad entry-point arguments");
+  Stream s;
+  TG_TRY(s.init());
+  return stage_cal_ep(dev_of(st), topm, ep, s.s);
+}
+
+int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const char* mode,
+                       const char* metric) {
+  TG_TRY(check_prune(p, st));
+  if (!mode || !metric) return fail(TAGORE_EINVAL, "null mode/metric");
+  Stream s;
+  TG_TRY(s.init());
+  Timer t;
+  t.start(s.s);
+  PruneArgs a{p->final_degree, p->topm, p->thre};
+  uint32_t ep = 0;
+  TG_TRY(prune_cfs(dev_of(st), a, mode, metric, &ep, s.s));
+  g_times.prune_ms = t.stop(s.s);
+  st->ep = ep;
+  return TAGORE_OK;
+}
+
+int tagore_pruning(const TagorePruneParams* p, TagoreKnnState* st, const char* index_type,
+                   const char* index_path) {
+  TG_TRY(check_prune(p, st));
+  if (!index_type) return fail(TAGORE_EINVAL, "null index_type");
+  const std::string type(index_type);
+  Stream s;
+  TG_TRY(s.init());
+  Timer t;
+  t.start(s.s);
+  PruneArgs a{p->final_degree, p->topm, p->thre};
+  uint32_t ep = 0;
+  TG_TRY(prune_index(dev_of(st), a, type, &ep, s.s));
+  g_times.prune_ms = t.stop(s.s);
+  st->ep = ep;
+  if (!index_path || !*index_path) return TAGORE_OK;
+  const uint32_t n = st->n, K = st->k, d = p->final_degree;
+  std::vector<uint32_t> rows((size_t)n * K);
+  TG_CUDA(cudaMemcpy(rows.data(), st->graph, rows.size() * 4, cudaMemcpyDeviceToHost));
+  if (type == "NSG") return tagore_store_nsg(index_path, rows.data(), d, ep, n, K);
+  if (type == "Vamana") return tagore_store_vamana(index_path, rows.data(), ep, n, K);
+  if (type == "NSSG") return tagore_store_nssg(index_path, rows.data(), d, n, K);
+  if (type == "CAGRA") return tagore_store_cagra(index_path, rows.data(), n, d);
+  return tagore_store_dpg(index_path, rows.data(), n, d);
+}
+
+int tagore_build_index_host(const TagoreKnnParams* p, const float* data, uint32_t n, uint32_t dim,
+                            uint32_t final_degree, uint32_t topm, float thre, uint32_t* out_graph,
+                            uint32_t* ep_out) {
+  if (!out_graph) return fail(TAGORE_EINVAL, "null output");
+  TagoreKnnState st{};
+  TG_TRY(tagore_gnn_descent_host(p, data, n, dim, &st));
+  TagorePruneParams pp{p->k, n, dim, final_degree, topm, thre};
+  int rc = tagore_pruning_cfs(&pp, &st, "path", "dist");
+  if (rc == TAGORE_OK) {
+    cudaError_t e = cudaMemcpy(out_graph, st.graph, (size_t)n * p->k * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(graph)", __FILE__, __LINE__);
+    if (ep_out) *ep_out = st.ep;
+  }
+  tagore_state_free(&st);
+  return rc;
+}
+
+int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev) {
+  (void)p;
+  (void)devices;
+  (void)ndev;
+  return fail(TAGORE_EINVAL, "largeIndex is not available in this build");
+}
+
+}  // extern "C"

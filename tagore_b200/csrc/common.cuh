@@ -1,0 +1,140 @@
+// common.cuh -- device helpers shared by the graph-build kernels (sm_100a).
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace tagore {
+
+constexpr uint32_t kInv = 0xFFFFFFFFu;
+constexpr float kInfDis = 10000000.0f;   // INF_DIS of the reference (include/common.cuh:29)
+constexpr uint32_t kReserve = 128;       // RESERVENUM: row stride of reverse_distance
+constexpr uint32_t kSelectCand = 480;    // SELECT_CAND: ring capacity of the path collect
+constexpr uint32_t kSample = 32;         // SAMPLE: hybrid_list rows are 4*SAMPLE wide
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ float2 h2lo(uint32_t v) {
+  return __half22float2(*reinterpret_cast<const __half2*>(&v));
+}
+
+// Accumulates one 4-dim chunk into the lane's (x, y) pair exactly as the
+// reference's two __hfma2 steps do (src/Tagore_src.cu:1431-1435), in FP32:
+// x takes dims 0 and 2, y takes dims 1 and 3, each a fused multiply-add of the
+// rounded difference.
+__device__ __forceinline__ void chunk_acc(uint2 a, uint2 b, float& x, float& y) {
+  const float2 a01 = h2lo(a.x), a23 = h2lo(a.y);
+  const float2 b01 = h2lo(b.x), b23 = h2lo(b.y);
+  const float d0 = __fsub_rn(a01.x, b01.x);
+  const float d1 = __fsub_rn(a01.y, b01.y);
+  const float d2 = __fsub_rn(a23.x, b23.x);
+  const float d3 = __fsub_rn(a23.y, b23.y);
+  x = __fmaf_rn(d0, d0, x);
+  y = __fmaf_rn(d1, d1, y);
+  x = __fmaf_rn(d2, d2, x);
+  y = __fmaf_rn(d3, d3, y);
+}
+
+// Reduces the per-lane pairs with the reference's shuffle-down tree (offsets
+// 16..1) and returns x + y in every lane.
+__device__ __forceinline__ float warp_tree(float x, float y) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    x = __fadd_rn(x, __shfl_down_sync(kFull, x, off));
+    y = __fadd_rn(y, __shfl_down_sync(kFull, y, off));
+  }
+  return __shfl_sync(kFull, __fadd_rn(x, y), 0);
+}
+
+// Exact FP32 squared L2 between two FP16 rows, in the reference's lane order.
+// Executed by a full warp; `dim` is a multiple of 4.
+__device__ __forceinline__ float warp_dist(const __half* __restrict__ a, const __half* __restrict__ b,
+                                           uint32_t dim, int lane) {
+  float x = 0.0f, y = 0.0f;
+  const uint32_t chunks = dim >> 2;
+  for (uint32_t j = lane; j < chunks; j += 32) {
+    const uint2 va = __ldg(reinterpret_cast<const uint2*>(a) + j);
+    const uint2 vb = __ldg(reinterpret_cast<const uint2*>(b) + j);
+    chunk_acc(va, vb, x, y);
+  }
+  return warp_tree(x, y);
+}
+
+// Four independent distances against one query, interleaving their shuffle
+// trees. Rows with id kInv yield 0 and must be ignored by the caller.
+__device__ __forceinline__ void warp_dist4(const __half* __restrict__ q, const __half* __restrict__ base,
+                                           uint32_t dim, const uint32_t ids[4], float out[4],
+                                           int lane) {
+  float x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f};
+  const uint32_t chunks = dim >> 2;
+  for (uint32_t j = lane; j < chunks; j += 32) {
+    const uint2 vq = *(reinterpret_cast<const uint2*>(q) + j);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      if (ids[t] != kInv) {
+        const uint2 vb = __ldg(reinterpret_cast<const uint2*>(base + (size_t)ids[t] * dim) + j);
+        chunk_acc(vq, vb, x[t], y[t]);
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      x[t] = __fadd_rn(x[t], __shfl_down_sync(kFull, x[t], off));
+      y[t] = __fadd_rn(y[t], __shfl_down_sync(kFull, y[t], off));
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) out[t] = __shfl_sync(kFull, __fadd_rn(x[t], y[t]), 0);
+}
+
+// distance_filter (src/Tagore_src.cu:1488-1490) as nvcc compiles it, one fused
+// multiply-add, and angle_filter (:1493-1495) with IEEE-rounded operations.
+__device__ __forceinline__ bool pruned_by(int metric, float res, float dis, float cur, float thre) {
+  if (metric == 0) return __fmaf_rn(thre, res, -dis) < 0.0f;
+  float v = __fsub_rn(__fadd_rn(dis, cur), res);
+  v = __fdiv_rn(v, 2.0f);
+  v = __fdiv_rn(v, __fsqrt_rn(__fmul_rn(dis, cur)));
+  return __fsub_rn(thre, v) < 0.0f;
+}
+
+// The reference's block-wide bitonic network (src/Tagore_src.cu:29-44),
+// executed by one warp over shared arrays: strides 1,2,4,.., steps stride..1,
+// the first step of each merge mirrored, pairs past `len` skipped. Each pass
+// touches disjoint pairs, so lane order inside a pass does not matter; the
+// swap sequence, and therefore tie placement, equals the reference's.
+template <class Gt, class Sw>
+__device__ __forceinline__ void warp_network(uint32_t len, int lane, Gt gt, Sw sw) {
+  for (uint32_t stride = 1; stride < len; stride <<= 1) {
+    for (uint32_t step = stride; step > 0; step >>= 1) {
+      const uint32_t sh = __ffs(step) - 1;
+      for (uint32_t k = lane; k < (len >> 1); k += 32) {
+        const uint32_t a = (k >> sh) << (sh + 1), b = k & (step - 1);
+        const uint32_t u = (step == stride) ? (a + step - 1 - b) : (a + b);
+        const uint32_t d = a + b + step;
+        if (d < len && gt(u, d)) sw(u, d);
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Lower-bound membership test in a sorted shared array.
+__device__ __forceinline__ bool sorted_contains(const uint32_t* a, uint32_t len, uint32_t key) {
+  uint32_t lo = 0, hi = len;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (a[mid] < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < len && a[lo] == key;
+}
+
+template <class T>
+__device__ __forceinline__ void swap_(T& a, T& b) {
+  T t = a;
+  a = b;
+  b = t;
+}
+
+}  // namespace tagore

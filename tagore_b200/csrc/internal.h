@@ -1,0 +1,108 @@
+// internal.h -- host-side interfaces between the C ABI and the kernel files.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/tagore_b200.h"
+
+namespace tagore {
+
+// Records a formatted message for tagore_last_error() and returns `code`.
+int fail(int code, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+#define TG_CUDA(call)                                                   \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess) return ::tagore::cuda_fail(e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define TG_TRY(expr)            \
+  do {                          \
+    int rc_ = (expr);           \
+    if (rc_ != TAGORE_OK) return rc_; \
+  } while (0)
+
+// Typed view of the eight reference buffers (capsule order, pybind.cu:132-141).
+struct Dev {
+  uint32_t n, k, dim;
+  uint32_t* graph;     // u32 [n*k]
+  uint32_t* rgraph;    // u32 [n*128]
+  __half* data;        // f16 [n*dim]
+  float* nd;           // f32 [n*k]
+  float* rd;           // f32 [n*128]
+  uint32_t* rnum;      // u32 [n]
+  __half* center;      // f16 [dim]
+  uint32_t* hybrid;    // u32 [n*128]
+};
+
+inline Dev dev_of(const TagoreKnnState* s) {
+  return Dev{s->n, s->k, s->dim, (uint32_t*)s->graph, (uint32_t*)s->reverse_graph,
+             (__half*)s->data, (float*)s->nei_distance, (float*)s->reverse_distance,
+             (uint32_t*)s->reverse_num, (__half*)s->center, (uint32_t*)s->hybrid_list};
+}
+
+// Stream-ordered device scratch that frees itself.
+struct Scratch {
+  cudaStream_t s;
+  void* p = nullptr;
+  explicit Scratch(cudaStream_t st) : s(st) {}
+  int alloc(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMallocAsync(&p, bytes, s);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return cuda_fail(e, "cudaMallocAsync(scratch)", __FILE__, __LINE__);
+    }
+    return TAGORE_OK;
+  }
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(p); }
+  ~Scratch() {
+    if (p) cudaFreeAsync(p, s);
+  }
+  Scratch(const Scratch&) = delete;
+  Scratch& operator=(const Scratch&) = delete;
+};
+
+// ---- prune (prune.cu) ----
+struct PruneArgs {
+  uint32_t final_degree, topm;
+  float thre;
+};
+// Pruning (pybind.cu:145-229) minus the file write. `type` is NSG, Vamana,
+// NSSG, CAGRA or DPG. Writes the entry point to *ep_host for NSG/Vamana.
+int prune_index(const Dev& d, const PruneArgs& a, const std::string& type, uint32_t* ep_host,
+                cudaStream_t s);
+// Pruning_with_CFS (pybind.cu:232-295).
+int prune_cfs(const Dev& d, const PruneArgs& a, const std::string& mode, const std::string& metric,
+              uint32_t* ep_host, cudaStream_t s);
+// Individual stages, exposed for the stage-level parity tests.
+int stage_cal_ep(const Dev& d, uint32_t topm, uint32_t* ep_host, cudaStream_t s);
+
+// ---- kNN graph (knn.cu) ----
+struct KnnArgs {
+  uint32_t k, iters, mode;  // mode: TAGORE_KNN_CHOSEN / TAGORE_KNN_PLAIN
+  uint32_t sample;          // forward samples per list per iteration
+  uint32_t per_row;         // proposals kept per join row
+  uint64_t seed;
+};
+struct KnnStats {
+  double ms_total, ms_prep, ms_iters;
+  uint64_t proposals, pairs;
+};
+// Builds the kNN graph over d.data (FP16 base) into d.graph / d.nd.
+int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, cudaStream_t s);
+
+// ---- base preparation (prep.cu) ----
+// FP16 base = raw * factor (as __float2half) and exact FP32 squared norms of
+// the FP16 rows, from the FP32 input already on the device.
+int prep_base(const float* raw, uint32_t n, uint32_t dim, float factor, __half* data, float* norms,
+              cudaStream_t s);
+float host_factor(const float* x, uint32_t dim, bool rescale);
+void host_center(const float* x, uint32_t n, uint32_t dim, float factor, uint16_t* center_half);
+
+}  // namespace tagore

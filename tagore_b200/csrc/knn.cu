@@ -1,0 +1,412 @@
+// knn.cu -- GNN-Descent style kNN graph construction on sm_100a.
+//
+// Replaces the two phases of the reference (src/Tagore_src.cu:158-1206,
+// driven from pybind.cu:103-125) by one NN-Descent loop over a packed 64-bit
+// neighbour pool:
+//   entry key = (float bits of the exact distance << 32) | (id << 1) | is_new
+// so a row sorted by key is sorted by distance, equal ids with equal distance
+// sit side by side (dedupe), and atomicMin on a key keeps the closer one.
+// Per iteration:
+//   sample  -- first S new and first S old entries of each row (the reference's
+//              split, :536-567), new ones marked old; reverse samples appended
+//              to the sampled nodes (:570-586);
+//   lists   -- each node's join list: forward+reverse new ids, then old ids;
+//   join    -- local join of new x (new u old); each list row keeps its
+//              `per_row` closest partners and proposes those closer than its
+//              current k-th entry by atomicMin into a hashed pool;
+//   merge   -- pool entries merged into the sorted row with a warp bitonic sort.
+// The join has two implementations: the plain one computes every pair with
+// FP32 SIMT arithmetic; the chosen one (knn_tc.cu) screens pairs on tcgen05
+// tensor-core tiles and re-ranks the kept ones exactly. Every stored distance
+// is the exact FP32 value in the reference's lane order, the same function the
+// prune stage uses.
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+#include "knn_shared.cuh"
+
+namespace tagore {
+namespace knn {
+
+__device__ __forceinline__ uint32_t mix32(uint64_t x) {
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdull;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ull;
+  x ^= x >> 33;
+  return (uint32_t)x;
+}
+
+// Random initial rows (the reference's initialize_graph, :158-166, seeded
+// instead of clock-seeded) with exact distances, sorted, repeats removed.
+__global__ void __launch_bounds__(128)
+    k_init(const __half* __restrict__ data, uint32_t n, uint32_t dim, uint32_t K, uint64_t seed,
+           uint64_t* __restrict__ nb) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t u = blockIdx.x * 4 + warp; u < n; u += gridDim.x * 4) {
+    uint64_t keys[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint32_t j = lane + 32 * t;
+      keys[t] = kEmpty;
+      if (j < K) {
+        uint32_t v = mix32(seed ^ ((uint64_t)u * 0x9E3779B97F4A7C15ull) ^ ((uint64_t)j << 40)) % (n - 1);
+        if (v >= u) ++v;  // never u itself
+        keys[t] = (uint64_t)v;
+      }
+    }
+    for (int t = 0; t < 4; ++t) {
+      for (int l0 = 0; l0 < 32; l0 += 4) {
+        uint32_t ids[4];
+        float d4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint64_t k = shfl_u64(keys[t], l0 + q);
+          ids[q] = (k == kEmpty) ? kInv : (uint32_t)k;
+        }
+        warp_dist4(data + (size_t)u * dim, data, dim, ids, d4, lane);
+        const int q = lane - l0;
+        if (q >= 0 && q < 4 && keys[t] != kEmpty) keys[t] = make_key(d4[q], (uint32_t)keys[t], true);
+      }
+    }
+    warp_sort_keys<4>(keys, lane);
+    dedupe_store_row<4>(keys, lane, nb + (size_t)u * K, K);
+  }
+}
+
+// First S new and first S old entries of each row; new ones become old.
+// Reverse samples are appended to the sampled nodes' lists (capacity S).
+__global__ void __launch_bounds__(128)
+    k_sample(uint64_t* __restrict__ nb, uint32_t n, uint32_t K, uint32_t S,
+             uint32_t* __restrict__ fnew, uint32_t* __restrict__ fold, uint32_t* __restrict__ fcnt,
+             uint32_t* __restrict__ rnew, uint32_t* __restrict__ rold,
+             uint32_t* __restrict__ rcnt) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t u = blockIdx.x * 4 + warp; u < n; u += gridDim.x * 4) {
+    uint64_t* row = nb + (size_t)u * K;
+    uint32_t cn = 0, co = 0;
+    for (uint32_t base = 0; base < K; base += 32) {
+      const uint32_t j = base + lane;
+      const uint64_t k = (j < K) ? row[j] : kEmpty;
+      const bool valid = k != kEmpty;
+      const bool isnew = valid && (k & 1ull);
+      const bool isold = valid && !(k & 1ull);
+      const unsigned mn = __ballot_sync(kFull, isnew), mo = __ballot_sync(kFull, isold);
+      const uint32_t rn = cn + __popc(mn & lt), ro = co + __popc(mo & lt);
+      if (isnew && rn < S) {
+        fnew[(size_t)u * S + rn] = key_id(k);
+        row[j] = k & ~1ull;
+      }
+      if (isold && ro < S) fold[(size_t)u * S + ro] = key_id(k);
+      cn += __popc(mn);
+      co += __popc(mo);
+    }
+    cn = min(cn, S);
+    co = min(co, S);
+    __syncwarp();
+    if (lane == 0) {
+      fcnt[2 * u] = cn;
+      fcnt[2 * u + 1] = co;
+    }
+    for (uint32_t i = lane; i < cn + co; i += 32) {
+      const bool isnew = i < cn;
+      const uint32_t v = isnew ? fnew[(size_t)u * S + i] : fold[(size_t)u * S + (i - cn)];
+      const uint32_t slot = atomicAdd(&rcnt[2 * v + (isnew ? 0 : 1)], 1u);
+      if (slot < S) (isnew ? rnew : rold)[(size_t)v * S + slot] = u;
+    }
+  }
+}
+
+// Join list of each node: forward new, reverse new (deduped, first kept),
+// then forward old and reverse old not already present. Warp per node.
+__global__ void __launch_bounds__(128)
+    k_build_lists(uint32_t n, uint32_t S, const uint32_t* __restrict__ fnew,
+                  const uint32_t* __restrict__ fold, const uint32_t* __restrict__ fcnt,
+                  const uint32_t* __restrict__ rnew, const uint32_t* __restrict__ rold,
+                  const uint32_t* __restrict__ rcnt, uint32_t* __restrict__ lists,
+                  uint32_t* __restrict__ lcnt) {
+  __shared__ uint32_t raw_all[4][4 * kMaxS];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  uint32_t* raw = raw_all[warp];
+  for (uint32_t u = blockIdx.x * 4 + warp; u < n; u += gridDim.x * 4) {
+    const uint32_t a = fcnt[2 * u], b = min(rcnt[2 * u], S);
+    const uint32_t c = fcnt[2 * u + 1], e = min(rcnt[2 * u + 1], S);
+    const uint32_t nraw = a + b, total_raw = a + b + c + e;
+    for (uint32_t i = lane; i < total_raw; i += 32) {
+      uint32_t v;
+      if (i < a) v = fnew[(size_t)u * S + i];
+      else if (i < a + b) v = rnew[(size_t)u * S + (i - a)];
+      else if (i < a + b + c) v = fold[(size_t)u * S + (i - a - b)];
+      else v = rold[(size_t)u * S + (i - a - b - c)];
+      raw[i] = v;
+    }
+    __syncwarp();
+    uint32_t keep_mask[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint32_t i = lane + 32 * t;
+      bool keep = false;
+      if (i < total_raw) {
+        const uint32_t v = raw[i];
+        keep = v != u;
+        for (uint32_t j = 0; j < i && keep; ++j) keep = raw[j] != v;
+      }
+      keep_mask[t] = keep ? 1u : 0u;
+    }
+    // ordered compaction: kept new entries first, then kept old entries
+    uint32_t pos = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const uint32_t i = lane + 32 * t;
+        const bool in_pass = pass == 0 ? (i < nraw) : (i >= nraw && i < total_raw);
+        const bool k = keep_mask[t] && in_pass;
+        const unsigned m = __ballot_sync(kFull, k);
+        if (k) lists[(size_t)u * kMaxList + pos + __popc(m & lt)] = raw[i];
+        pos += __popc(m);
+      }
+      if (pass == 0 && lane == 0) lcnt[2 * u] = pos;
+    }
+    if (lane == 0) lcnt[2 * u + 1] = pos;
+    __syncwarp();
+  }
+}
+
+// Plain local join: every pair with a new endpoint computed once with FP32
+// SIMT arithmetic (thread per pair, reference lane order), kept in a shared
+// distance matrix; each row then proposes its `per_row` closest partners.
+template <int D>
+__global__ void __launch_bounds__(128)
+    k_join_plain(const uint64_t* __restrict__ nb, const __half* __restrict__ data, uint32_t n,
+                 uint32_t dim_rt, uint32_t K, uint32_t T, uint32_t P,
+                 const uint32_t* __restrict__ lists, const uint32_t* __restrict__ lcnt,
+                 unsigned long long* __restrict__ pool, unsigned long long* __restrict__ stats) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const uint32_t dim = D > 0 ? (uint32_t)D : dim_rt;
+  const uint32_t words = dim / 2 + 1;  // padded row stride in 32-bit words
+  uint32_t* list = reinterpret_cast<uint32_t*>(smem);  // 128
+  float* kth = reinterpret_cast<float*>(list + kMaxList);  // 128
+  float* dm = kth + kMaxList;  // 128 x 129
+  uint32_t* vec = reinterpret_cast<uint32_t*>(dm + kMaxList * (kMaxList + 1));
+  const uint32_t tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  unsigned long long props = 0, pairs = 0;
+  for (uint32_t u = blockIdx.x; u < n; u += gridDim.x) {
+    const uint32_t nn = lcnt[2 * u], total = lcnt[2 * u + 1];
+    if (nn == 0 || total < 2) continue;
+    if (tid < total) {
+      list[tid] = lists[(size_t)u * kMaxList + tid];
+      kth[tid] = kth_of(nb[(size_t)list[tid] * K + K - 1]);
+    }
+    __syncthreads();
+    for (uint32_t r = warp; r < total; r += 4) {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(data + (size_t)list[r] * dim);
+      for (uint32_t w = lane; w < dim / 2; w += 32) vec[r * words + w] = __ldg(src + w);
+    }
+    __syncthreads();
+    for (uint32_t r = 0; r < nn; ++r) {
+      for (uint32_t c = r + 1 + tid; c < total; c += blockDim.x) {
+        const float d = thread_dist<D>(vec + r * words, vec + c * words, dim);
+        dm[r * (kMaxList + 1) + c] = d;
+        dm[c * (kMaxList + 1) + r] = d;
+        ++pairs;
+      }
+    }
+    __syncthreads();
+    if (tid < total) {
+      const uint32_t r = tid;
+      float bd[kMaxT];
+      uint32_t bc[kMaxT];
+      for (uint32_t t = 0; t < T; ++t) {
+        bd[t] = __int_as_float(0x7f800000);
+        bc[t] = kInv;
+      }
+      for (uint32_t c = 0; c < total; ++c) {
+        if (c == r || (r >= nn && c >= nn)) continue;
+        float v = dm[r * (kMaxList + 1) + c];
+        uint32_t vc = c;
+        for (uint32_t t = 0; t < T; ++t)
+          if (v < bd[t]) {
+            swap_(v, bd[t]);
+            swap_(vc, bc[t]);
+          }
+      }
+      const uint32_t a = list[r];
+      for (uint32_t t = 0; t < T; ++t) {
+        if (bc[t] == kInv || !(bd[t] < kth[r])) break;
+        propose(pool, a, P, list[bc[t]], bd[t]);
+        ++props;
+      }
+    }
+    __syncthreads();
+  }
+  atomicAdd(&stats[0], props);
+  atomicAdd(&stats[1], pairs);
+}
+
+// Merges the pool of each node into its sorted row and clears the pool.
+__global__ void __launch_bounds__(128)
+    k_merge(uint64_t* __restrict__ nb, unsigned long long* __restrict__ pool, uint32_t n,
+            uint32_t K, uint32_t P, unsigned long long* __restrict__ stats) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long upd = 0;
+  for (uint32_t u = blockIdx.x * 4 + warp; u < n; u += gridDim.x * 4) {
+    uint64_t* row = nb + (size_t)u * K;
+    unsigned long long* pl = pool + (size_t)u * P;
+    const uint64_t kth = row[K - 1];
+    uint64_t keys[8];
+    // positions 0..127 hold the row (K <= 128), 128..255 the pool (P <= 128)
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint32_t j = lane + 32 * t;
+      keys[t] = (j < K) ? row[j] : kEmpty;
+    }
+    uint32_t fresh = 0;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint32_t j = lane + 32 * t;
+      uint64_t k = kEmpty;
+      if (j < P) {
+        k = pl[j];
+        if (k != kEmpty) pl[j] = kEmpty;
+        if (!(k < kth)) k = kEmpty;
+        else ++fresh;
+      }
+      keys[4 + t] = k;
+    }
+    if (__reduce_add_sync(kFull, fresh) == 0) continue;
+    warp_sort_keys<8>(keys, lane);
+    upd += dedupe_store_row<8>(keys, lane, row, K);
+  }
+  if (lane == 0) atomicAdd(&stats[2], upd);
+}
+
+// Splits the packed rows into the reference's graph (u32) and nei_distance
+// (f32) buffers; an empty slot repeats the row's first id.
+__global__ void k_finalize(const uint64_t* __restrict__ nb, uint32_t n, uint32_t K,
+                           uint32_t* __restrict__ graph, float* __restrict__ nd) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)n * K;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const uint64_t k = nb[e];
+    const size_t r0 = e - e % K;
+    if (k == kEmpty) {
+      const uint64_t f = nb[r0];
+      graph[e] = (f == kEmpty) ? (uint32_t)((e / K + 1) % n) : key_id(f);
+      nd[e] = kInfDis;
+    } else {
+      graph[e] = key_id(k);
+      nd[e] = key_dist(k);
+    }
+  }
+}
+
+int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+template <int D>
+int launch_join_plain(const Work& w, cudaStream_t s) {
+  const uint32_t words = w.dim / 2 + 1;
+  const size_t sm = (size_t)2 * kMaxList * 4 + (size_t)kMaxList * (kMaxList + 1) * 4 +
+                    (size_t)kMaxList * words * 4;
+  if (sm > 227 * 1024) return fail(TAGORE_EINVAL, "plain join: DIM %u too large", w.dim);
+  TG_CUDA(cudaFuncSetAttribute((const void*)k_join_plain<D>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const int grid = sm_count() * std::max(1, (int)((227 * 1024) / (sm + 1024)));
+  k_join_plain<D><<<grid, 128, sm, s>>>(w.nb, w.data, w.n, w.dim, w.K, w.T, w.P, w.lists, w.lcnt,
+                                        w.pool, w.stats);
+  TG_CUDA(cudaGetLastError());
+  return TAGORE_OK;
+}
+
+int join_plain(const Work& w, cudaStream_t s) {
+  switch (w.dim) {
+    case 96: return launch_join_plain<96>(w, s);
+    case 128: return launch_join_plain<128>(w, s);
+    default: return launch_join_plain<0>(w, s);
+  }
+}
+
+}  // namespace knn
+
+int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, cudaStream_t s) {
+  using namespace knn;
+  if (d.n < 2 || a.k == 0 || a.k >= d.n) return fail(TAGORE_EINVAL, "need POINTS > K >= 1");
+  if (a.k > 128) return fail(TAGORE_EINVAL, "K must be <= 128 (got %u)", a.k);
+  if (d.dim % 4) return fail(TAGORE_EINVAL, "DIM must be a multiple of 4 (got %u)", d.dim);
+  if (d.n >= 0x7FFFFFFFu) return fail(TAGORE_EINVAL, "POINTS must be < 2^31");
+  const uint32_t S = std::min<uint32_t>(a.sample ? a.sample : 32, kMaxS);
+  const uint32_t T = std::min<uint32_t>(a.per_row ? a.per_row : 2,
+                                        a.mode == TAGORE_KNN_PLAIN ? kMaxT : 4u);
+  const uint32_t P = kPool;
+  const uint32_t K = a.k;
+  Work w{};
+  w.n = d.n;
+  w.dim = d.dim;
+  w.K = K;
+  w.S = S;
+  w.T = T;
+  w.P = P;
+  w.data = d.data;
+  w.norms = norms;
+  const size_t nbB = (size_t)d.n * K * 8, poolB = (size_t)d.n * P * 8;
+  const size_t listB = (size_t)d.n * S * 4;
+  Scratch sc(s);
+  TG_TRY(sc.alloc(nbB + poolB + 4 * listB + (size_t)d.n * kMaxList * 4 + (size_t)d.n * 24 + 128));
+  unsigned char* p = sc.as<unsigned char>();
+  w.nb = reinterpret_cast<uint64_t*>(p);
+  p += nbB;
+  w.pool = reinterpret_cast<unsigned long long*>(p);
+  p += poolB;
+  w.fnew = reinterpret_cast<uint32_t*>(p);
+  w.fold = w.fnew + (size_t)d.n * S;
+  w.rnew = w.fold + (size_t)d.n * S;
+  w.rold = w.rnew + (size_t)d.n * S;
+  w.lists = w.rold + (size_t)d.n * S;
+  w.fcnt = w.lists + (size_t)d.n * kMaxList;
+  w.rcnt = w.fcnt + (size_t)d.n * 2;
+  w.lcnt = w.rcnt + (size_t)d.n * 2;
+  w.stats = reinterpret_cast<unsigned long long*>(
+      (reinterpret_cast<uintptr_t>(w.lcnt + (size_t)d.n * 2) + 15) & ~(uintptr_t)15);
+  TG_CUDA(cudaMemsetAsync(w.pool, 0xFF, poolB, s));
+  TG_CUDA(cudaMemsetAsync(w.stats, 0, 64, s));
+  const int sms = sm_count();
+  k_init<<<sms * 16, 128, 0, s>>>(d.data, d.n, d.dim, K, a.seed, w.nb);
+  TG_CUDA(cudaGetLastError());
+  for (uint32_t it = 0; it < a.iters; ++it) {
+    TG_CUDA(cudaMemsetAsync(w.rcnt, 0, (size_t)d.n * 8, s));
+    k_sample<<<sms * 16, 128, 0, s>>>(w.nb, d.n, K, S, w.fnew, w.fold, w.fcnt, w.rnew, w.rold,
+                                       w.rcnt);
+    TG_CUDA(cudaGetLastError());
+    k_build_lists<<<sms * 16, 128, 0, s>>>(d.n, S, w.fnew, w.fold, w.fcnt, w.rnew, w.rold, w.rcnt,
+                                           w.lists, w.lcnt);
+    TG_CUDA(cudaGetLastError());
+    if (a.mode == TAGORE_KNN_PLAIN) {
+      TG_TRY(join_plain(w, s));
+    } else {
+      TG_TRY(join_tc(w, s));
+    }
+    k_merge<<<sms * 16, 128, 0, s>>>(w.nb, w.pool, d.n, K, P, w.stats);
+    TG_CUDA(cudaGetLastError());
+  }
+  k_finalize<<<sms * 8, 256, 0, s>>>(w.nb, d.n, K, d.graph, d.nd);
+  TG_CUDA(cudaGetLastError());
+  unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  TG_CUDA(cudaMemcpyAsync(h, w.stats, sizeof(h), cudaMemcpyDeviceToHost, s));
+  TG_CUDA(cudaStreamSynchronize(s));
+  if ((uint32_t)h[4] != 0) return fail(TAGORE_ETIMEOUT, "tensor-core join: a bounded wait ran out");
+  if (st) {
+    st->proposals = h[0];
+    st->pairs = h[1];
+  }
+  return TAGORE_OK;
+}
+
+}  // namespace tagore

@@ -1,0 +1,908 @@
+// prune.cu -- Collect / Filter / Store prune of a kNN graph on sm_100a.
+//
+// Restates the CFS framework of ZJU-DAILY/Tagore (src/Tagore_src.cu:1209-2058,
+// pybind.cu:145-295) with one warp per node and results that are a function of
+// the input graph only:
+//  * every distance is FP32 arithmetic on the FP16 base in the reference's
+//    lane order (common.cuh), every sort is the reference's bitonic network on
+//    the same positions, so ties fall where the reference puts them;
+//  * the Collect stage reads the kNN graph as a snapshot: pruned rows go to
+//    scratch and reach `graph` only in the Store stage;
+//  * reverse edges are inserted in ascending source order (a stable radix sort
+//    by target), so the reference's replacement rule for full lists
+//    (:1465-1475, :1697-1707) gives one defined answer;
+//  * the Filter stage is evaluated lazily: a candidate is tested against the
+//    kept neighbours in order and dropped at the first rule that fires, which
+//    keeps exactly the set the reference's round-by-round sweep (:1416-1460)
+//    keeps while computing far fewer distances.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace tagore {
+namespace {
+
+constexpr int kWarps = 4;  // warps (= nodes in flight) per block
+
+__device__ __forceinline__ uint32_t align4(uint32_t x) { return (x + 3u) & ~3u; }
+
+// ---------------------------------------------------------------------------
+// Beam search shared by cal_ep_gpu (:1905-2047) and collect_path (:1211-1335).
+struct Beam {
+  uint32_t* id;
+  float* dis;
+  uint32_t* id2;
+  uint8_t* ex;
+};
+
+__device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __restrict__ data,
+                              uint32_t dim, uint32_t K, const __half* query, uint32_t start,
+                              uint32_t topm, uint32_t iters, Beam bm, uint32_t* ring_id,
+                              float* ring_dis, uint32_t* ring_count, int lane) {
+  const uint32_t W = topm + K;
+  for (uint32_t t = lane; t < W; t += 32) {
+    bm.id[t] = kInv;
+    bm.dis[t] = kInfDis;
+    bm.ex[t] = 1;
+  }
+  __syncwarp();
+  for (uint32_t t = lane; t < K; t += 32) {
+    bm.id[topm + t] = __ldg(G + (size_t)start * K + t);
+    bm.ex[topm + t] = 0;
+  }
+  __syncwarp();
+  for (uint32_t i = 0; i < K; i += 4) {
+    uint32_t ids[4];
+    float d4[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) ids[t] = (i + t < K) ? bm.id[topm + i + t] : kInv;
+    warp_dist4(query, data, dim, ids, d4, lane);
+    if (lane == 0) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if (i + t < K) {
+          bm.dis[topm + i + t] = d4[t];
+          if (ring_id) {
+            ring_id[(i + t) % kSelectCand] = ids[t];
+            ring_dis[(i + t) % kSelectCand] = d4[t];
+          }
+        }
+    }
+  }
+  __syncwarp();
+  {
+    float* D = bm.dis + topm;
+    uint32_t* I = bm.id + topm;
+    uint8_t* E = bm.ex + topm;
+    warp_network(K, lane, [&](uint32_t u, uint32_t d) { return D[u] > D[d]; },
+                 [&](uint32_t u, uint32_t d) {
+                   swap_(D[u], D[d]);
+                   swap_(I[u], I[d]);
+                   swap_(E[u], E[d]);
+                 });
+  }
+  for (uint32_t i = lane; i < topm; i += 32) {
+    if (topm + i < W) {
+      bm.id[i] = bm.id[topm + i];
+      bm.dis[i] = bm.dis[topm + i];
+      bm.ex[i] = bm.ex[topm + i];
+    } else {  // slots past the K seeds start empty (TOPM > K)
+      bm.id[i] = kInv;
+      bm.dis[i] = kInfDis;
+      bm.ex[i] = 1;
+    }
+  }
+  __syncwarp();
+  auto rebuild_id2 = [&]() {
+    for (uint32_t t = lane; t < W; t += 32) bm.id2[t] = bm.id[t];
+    __syncwarp();
+    warp_network(W, lane, [&](uint32_t u, uint32_t d) { return bm.id2[u] > bm.id2[d]; },
+                 [&](uint32_t u, uint32_t d) { swap_(bm.id2[u], bm.id2[d]); });
+  };
+  rebuild_id2();
+  uint32_t curr = K, to_explore = kInv;
+  for (uint32_t it = 0; it < iters; ++it) {
+    // First unexplored of the top TOPM; when none is left the reference keeps
+    // the previous node (its `j == TOPM` test never fires, :1270).
+    for (uint32_t base = 0; base < topm; base += 32) {
+      const uint32_t j = base + lane;
+      const unsigned m = __ballot_sync(kFull, j < topm && !bm.ex[j]);
+      if (m) {
+        const uint32_t f = base + __ffs(m) - 1;
+        to_explore = bm.id[f];
+        __syncwarp();
+        if (lane == 0) bm.ex[f] = 1;
+        break;
+      }
+    }
+    __syncwarp();
+    if (to_explore == kInv) break;
+    for (uint32_t j = lane; j < K; j += 32) {
+      const uint32_t a = __ldg(G + (size_t)to_explore * K + j);
+      bm.dis[topm + j] = sorted_contains(bm.id2, W, a) ? kInfDis : 0.0f;
+      bm.id[topm + j] = a;
+      bm.ex[topm + j] = 0;
+    }
+    __syncwarp();
+    // Distances of the non-members in ascending neighbour order; that order
+    // also fixes their ring slots.
+    uint32_t pend[4];
+    int np = 0;
+    auto flush = [&]() {
+      uint32_t ids[4];
+      float d4[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) ids[t] = (t < np) ? bm.id[topm + pend[t]] : kInv;
+      warp_dist4(query, data, dim, ids, d4, lane);
+      if (lane == 0) {
+        for (int t = 0; t < np; ++t) {
+          bm.dis[topm + pend[t]] = d4[t];
+          if (ring_id) {
+            ring_id[(curr + t) % kSelectCand] = ids[t];
+            ring_dis[(curr + t) % kSelectCand] = d4[t];
+          }
+        }
+      }
+      curr += np;
+      np = 0;
+    };
+    for (uint32_t base = 0; base < K; base += 32) {
+      const uint32_t j = base + lane;
+      unsigned m = __ballot_sync(kFull, j < K && bm.dis[topm + j] < 1.0f);
+      while (m) {
+        pend[np++] = base + __ffs(m) - 1;
+        m &= m - 1;
+        if (np == 4) flush();
+      }
+    }
+    if (np) flush();
+    __syncwarp();
+    warp_network(W, lane, [&](uint32_t u, uint32_t d) { return bm.dis[u] > bm.dis[d]; },
+                 [&](uint32_t u, uint32_t d) {
+                   swap_(bm.dis[u], bm.dis[d]);
+                   swap_(bm.id[u], bm.id[d]);
+                   swap_(bm.ex[u], bm.ex[d]);
+                 });
+    rebuild_id2();
+  }
+  if (ring_count) *ring_count = curr;
+  return bm.id[0];
+}
+
+// Sort by distance with the reference network, then mark adjacent repeats
+// using the ids as they were before marking (:1345-1348).
+__device__ void warp_sort_mark(uint32_t* cand, float* dis, uint32_t len, int lane) {
+  warp_network(len, lane, [&](uint32_t u, uint32_t d) { return dis[u] > dis[d]; },
+               [&](uint32_t u, uint32_t d) {
+                 swap_(dis[u], dis[d]);
+                 swap_(cand[u], cand[d]);
+               });
+  // Two passes: decide from the unmarked ids, then mark.
+  unsigned marks[(kSelectCand + 128 + 31) / 32];
+  const uint32_t chunks = (len + 31) / 32;
+  for (uint32_t c = 0; c < chunks; ++c) {
+    const uint32_t i = c * 32 + lane;
+    const bool rep = i >= 1 && i < len && cand[i] == cand[i - 1];
+    marks[c] = __ballot_sync(kFull, rep);
+  }
+  __syncwarp();
+  for (uint32_t c = 0; c < chunks; ++c)
+    if ((marks[c] >> lane) & 1u) cand[c * 32 + lane] = kInv;
+  __syncwarp();
+}
+
+// Filter stage, lazily evaluated (see file header). Returns the number of ids
+// the reference stores: one less than its selection steps (:1462, :1623).
+__device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_t len,
+                                uint32_t bid, uint32_t fd, int metric, float thre,
+                                const __half* __restrict__ data, uint32_t dim, uint32_t* sel,
+                                float* seld, int lane) {
+  uint32_t first = kInv;
+  for (uint32_t base = 0; base < len; base += 32) {
+    const uint32_t i = base + lane;
+    const bool ok = i < len && cand[i] != bid && cand[i] != kInv;
+    const unsigned m = __ballot_sync(kFull, ok);
+    if (m) {
+      first = base + __ffs(m) - 1;
+      break;
+    }
+  }
+  if (first == kInv) return 0;
+  if (lane == 0) {
+    sel[0] = cand[first];
+    seld[0] = cdis[first];
+  }
+  __syncwarp();
+  uint32_t nsel = 1, last_pos = first;
+  for (uint32_t i = first + 1; i < len && nsel < fd; ++i) {
+    const uint32_t c = cand[i];
+    if (c == kInv) continue;
+    bool dup = false;
+    for (uint32_t s0 = 0; s0 < nsel; s0 += 32) {
+      const uint32_t s = s0 + lane;
+      if (__any_sync(kFull, s < nsel && sel[s] == c)) {
+        dup = true;
+        break;
+      }
+    }
+    if (dup) continue;
+    const float dc = cdis[i];
+    const __half* cv = data + (size_t)c * dim;
+    bool pruned = false;
+    for (uint32_t s = 0; s < nsel && !pruned; s += 4) {
+      uint32_t ids[4];
+      float r4[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) ids[t] = (s + t < nsel) ? sel[s + t] : kInv;
+      warp_dist4(cv, data, dim, ids, r4, lane);
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if (!pruned && s + t < nsel) pruned = pruned_by(metric, r4[t], dc, seld[s + t], thre);
+    }
+    if (!pruned) {
+      if (lane == 0) {
+        sel[nsel] = c;
+        seld[nsel] = dc;
+      }
+      __syncwarp();
+      ++nsel;
+      last_pos = i;
+    }
+  }
+  __syncwarp();
+  if (nsel == fd) return fd - 1;
+  if (nsel >= 2 && last_pos == len - 1) return nsel - 1;
+  return nsel;
+}
+
+// Per-warp shared layout of the select kernels.
+struct SelLayout {
+  uint32_t W, L, fd;
+  __host__ __device__ size_t bytes() const {
+    return (size_t)W * 12 + ((W + 15u) & ~15u) + (size_t)L * 8 + (size_t)fd * 8 + 64;
+  }
+};
+
+// ---------------------------------------------------------------------------
+__global__ void k_validate(const uint32_t* __restrict__ g, size_t cnt, uint32_t n,
+                           uint32_t* bad) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt;
+       i += (size_t)gridDim.x * blockDim.x)
+    if (g[i] >= n) atomicExch(bad, 1u);
+}
+
+// cal_ep_gpu (:1889-2058): one warp, 30 expansions from node 0 toward the centre.
+__global__ void k_cal_ep(const uint32_t* __restrict__ G, const __half* __restrict__ data,
+                         const __half* __restrict__ center, uint32_t dim, uint32_t K,
+                         uint32_t topm, uint32_t* ep) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const uint32_t W = topm + K;
+  Beam bm;
+  bm.id = reinterpret_cast<uint32_t*>(smem);
+  bm.dis = reinterpret_cast<float*>(bm.id + W);
+  bm.id2 = reinterpret_cast<uint32_t*>(bm.dis + W);
+  bm.ex = reinterpret_cast<uint8_t*>(bm.id2 + W);
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x >= 32) return;
+  const uint32_t best = warp_beam(G, data, dim, K, center, 0, topm, 30, bm, nullptr, nullptr,
+                                  nullptr, lane);
+  if (lane == 0) *ep = best;
+}
+
+// select_path (:1498-1517) and select_2hop (:1520-1534) into scratch rows.
+// path: collect_path + Filter_path(distance_filter); 2-hop: collect_2hop +
+// Filter_path(angle_filter). The reference always uses these two filters.
+template <bool kPath>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_select(const uint32_t* __restrict__ G, float* __restrict__ nd, const __half* __restrict__ data,
+             uint32_t n, uint32_t dim, uint32_t K, const uint32_t* __restrict__ ep_dev,
+             uint32_t topm, uint32_t fd, float thre, uint32_t* __restrict__ P_ids,
+             float* __restrict__ P_dis, uint32_t* __restrict__ P_cnt) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  SelLayout lay{kPath ? topm + K : 0u, kSelectCand + K, fd};
+  unsigned char* mine = smem + (size_t)warp * lay.bytes();
+  uint32_t* cand = reinterpret_cast<uint32_t*>(mine);
+  float* cdis = reinterpret_cast<float*>(cand + lay.L);
+  uint32_t* sel = reinterpret_cast<uint32_t*>(cdis + lay.L);
+  float* seld = reinterpret_cast<float*>(sel + fd);
+  Beam bm;
+  bm.id = reinterpret_cast<uint32_t*>(seld + fd);
+  bm.dis = reinterpret_cast<float*>(bm.id + lay.W);
+  bm.id2 = reinterpret_cast<uint32_t*>(bm.dis + lay.W);
+  bm.ex = reinterpret_cast<uint8_t*>(bm.id2 + lay.W);
+  const uint32_t L = lay.L;
+  const uint32_t ep = kPath ? *ep_dev : 0u;
+  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+    const __half* q = data + (size_t)b * dim;
+    if (kPath) {
+      uint32_t curr = 0;
+      warp_beam(G, data, dim, K, q, ep, topm, 10, bm, cand + K, cdis + K, &curr, lane);
+      for (uint32_t i = curr + lane; i < kSelectCand; i += 32) {
+        cand[K + i] = kInv;
+        cdis[K + i] = kInfDis;
+      }
+    } else {
+      for (uint32_t i = lane; i < kSelectCand; i += 32)
+        cand[K + i] = __ldg(G + (size_t)__ldg(G + (size_t)b * K + i / K) * K + i % K);
+      __syncwarp();
+      for (uint32_t i = 0; i < kSelectCand; i += 4) {
+        uint32_t ids[4];
+        float d4[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) ids[t] = cand[K + i + t];
+        warp_dist4(q, data, dim, ids, d4, lane);
+        if (lane == 0) {
+#pragma unroll
+          for (int t = 0; t < 4; ++t) cdis[K + i + t] = d4[t];
+        }
+      }
+    }
+    for (uint32_t i = lane; i < K; i += 32) {
+      cand[i] = __ldg(G + (size_t)b * K + i);
+      cdis[i] = nd[(size_t)b * K + i];
+    }
+    __syncwarp();
+    warp_sort_mark(cand, cdis, L, lane);
+    const uint32_t stored =
+        warp_filter(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel, seld, lane);
+    for (uint32_t i = lane; i < stored; i += 32) {
+      P_ids[(size_t)b * fd + i] = sel[i];
+      P_dis[(size_t)b * fd + i] = seld[i];
+      nd[(size_t)b * K + i] = seld[i];  // own row only: no other block reads it
+    }
+    if (lane == 0) P_cnt[b] = stored;
+    __syncwarp();
+  }
+}
+
+// filter_reverse (:1537-1657) plus the in-place row writes of the select
+// kernels (:1462-1464, :1477): the stored row is the kNN row overwritten by
+// the select result, then by this stage's result.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_filter_reverse(uint32_t* __restrict__ graph, const float* __restrict__ nd,
+                     const uint32_t* __restrict__ rg, const float* __restrict__ rd,
+                     const uint32_t* __restrict__ rnum, const __half* __restrict__ data,
+                     uint32_t n, uint32_t dim, uint32_t K, uint32_t fd, int metric, float thre,
+                     const uint32_t* __restrict__ P_ids, const uint32_t* __restrict__ P_cnt) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t cap = fd + K;  // cur_num <= fd - 1, rever_num <= K
+  unsigned char* mine = smem + (size_t)warp * ((size_t)cap * 8 + (size_t)fd * 8 + 16);
+  uint32_t* cand = reinterpret_cast<uint32_t*>(mine);
+  float* cdis = reinterpret_cast<float*>(cand + cap);
+  uint32_t* sel = reinterpret_cast<uint32_t*>(cdis + cap);
+  float* seld = reinterpret_cast<float*>(sel + fd);
+  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+    const uint32_t cur_num = P_cnt[b];
+    const uint32_t rn = min(K, rnum[b]);
+    const uint32_t len = cur_num + rn;
+    for (uint32_t i = lane; i < cur_num; i += 32) {
+      cand[i] = P_ids[(size_t)b * fd + i];
+      cdis[i] = nd[(size_t)b * K + i];
+    }
+    for (uint32_t i = lane; i < rn; i += 32) {
+      cand[cur_num + i] = rg[(size_t)b * K + i];
+      cdis[cur_num + i] = rd[(size_t)b * kReserve + i];
+    }
+    __syncwarp();
+    uint32_t* row = graph + (size_t)b * K;
+    uint32_t out_cnt;
+    if (len > fd) {
+      warp_sort_mark(cand, cdis, len, lane);
+      out_cnt = warp_filter(cand, cdis, len, b, fd, metric, thre, data, dim, sel, seld, lane);
+    } else {
+      // Union in ascending reverse-slot order (:1632-1647).
+      for (uint32_t i = lane; i < cur_num; i += 32) sel[i] = cand[i];
+      uint32_t dup = 0;
+      for (uint32_t i = 0; i < rn; ++i) {
+        const uint32_t r = cand[cur_num + i];
+        bool found = false;
+        for (uint32_t j0 = 0; j0 < cur_num; j0 += 32) {
+          const uint32_t j = j0 + lane;
+          if (__any_sync(kFull, j < cur_num && cand[j] == r)) {
+            found = true;
+            break;
+          }
+        }
+        // A stride-K row holds at most K-1 ids; with FINAL_DEGREE == K the
+        // reference would spill its last union id into the next row.
+        if (!found && cur_num + dup + 1 < K) {
+          if (lane == 0) sel[cur_num + dup] = r;
+          ++dup;
+        }
+      }
+      out_cnt = cur_num + dup;
+    }
+    __syncwarp();
+    const uint32_t top = max(out_cnt, cur_num);
+    for (uint32_t i = lane; i < top; i += 32)
+      row[i + 1] = (i < out_cnt) ? sel[i] : P_ids[(size_t)b * fd + i];
+    if (lane == 0) row[0] = out_cnt;
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Rank-based prunes. collect_1hop + filter_cagra (:1660-1710): detour[m]
+// counts the kept-earlier neighbours a whose own list holds n_m, over the
+// pairs the reference visits (a in {i, K-1-i : i < K/2}, m > a).
+__global__ void __launch_bounds__(kWarps * 32)
+    k_select_cagra(const uint32_t* __restrict__ G, uint32_t n, uint32_t K, uint32_t d,
+                   uint32_t* __restrict__ hybrid, uint32_t* __restrict__ E_tgt,
+                   uint32_t* __restrict__ E_val) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr uint32_t H = 256;  // hash slots, K <= 128 keeps the load <= 1/2
+  unsigned char* mine = smem + (size_t)warp * (H * 4 + (size_t)K * 8);
+  uint32_t* hash = reinterpret_cast<uint32_t*>(mine);
+  uint32_t* nei0 = hash + H;
+  uint32_t* det = nei0 + K;
+  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+    for (uint32_t j = lane; j < K; j += 32) {
+      nei0[j] = __ldg(G + (size_t)b * K + j);
+      det[j] = 0;
+    }
+    __syncwarp();
+    for (uint32_t i = 0; i < K / 2; ++i) {
+      for (int side = 0; side < 2; ++side) {
+        const uint32_t a = side ? (K - 1 - i) : i;
+        if (a + 1 >= K) continue;
+        for (uint32_t t = lane; t < H; t += 32) hash[t] = kInv;
+        __syncwarp();
+        const uint32_t* row = G + (size_t)nei0[a] * K;
+        for (uint32_t j = lane; j < K; j += 32) {
+          const uint32_t key = __ldg(row + j);
+          uint32_t h = (key * 0x9E3779B1u) >> 24;
+          while (true) {
+            const uint32_t prev = atomicCAS(&hash[h], kInv, key);
+            if (prev == kInv || prev == key) break;
+            h = (h + 1) & (H - 1);
+          }
+        }
+        __syncwarp();
+        for (uint32_t m = a + 1 + lane; m < K; m += 32) {
+          const uint32_t key = nei0[m];
+          uint32_t h = (key * 0x9E3779B1u) >> 24;
+          bool hit = false;
+          while (true) {
+            const uint32_t v = hash[h];
+            if (v == key) {
+              hit = true;
+              break;
+            }
+            if (v == kInv) break;
+            h = (h + 1) & (H - 1);
+          }
+          if (hit) det[m] += 1;  // m is owned by this lane
+        }
+        __syncwarp();
+      }
+    }
+    warp_network(K, lane, [&](uint32_t u, uint32_t v) { return det[u] > det[v]; },
+                 [&](uint32_t u, uint32_t v) {
+                   swap_(det[u], det[v]);
+                   swap_(nei0[u], nei0[v]);
+                 });
+    for (uint32_t i = lane; i < d; i += 32) {
+      E_tgt[(size_t)b * d + i] = nei0[i];
+      E_val[(size_t)b * d + i] = det[i];
+      hybrid[(size_t)b * K + i] = nei0[i];
+    }
+    __syncwarp();
+  }
+}
+
+// collect_1hop + filter_dpg (:1713-1785): detour[m] counts earlier a with
+// d(n_a, n_m) < d(u, n_m), each warp using its own vector (see header note).
+__global__ void __launch_bounds__(kWarps * 32)
+    k_select_dpg(const uint32_t* __restrict__ G, const float* __restrict__ nd,
+                 const __half* __restrict__ data, uint32_t n, uint32_t dim, uint32_t K, uint32_t d,
+                 uint32_t* __restrict__ hybrid, uint32_t* __restrict__ E_tgt,
+                 uint32_t* __restrict__ E_val) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned char* mine = smem + (size_t)warp * ((size_t)K * 12);
+  uint32_t* nei0 = reinterpret_cast<uint32_t*>(mine);
+  uint32_t* det = nei0 + K;
+  float* nrow = reinterpret_cast<float*>(det + K);
+  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+    for (uint32_t j = lane; j < K; j += 32) {
+      nei0[j] = __ldg(G + (size_t)b * K + j);
+      det[j] = 0;
+      nrow[j] = nd[(size_t)b * K + j];
+    }
+    __syncwarp();
+    for (uint32_t i = 0; i < K / 2; ++i) {
+      for (int side = 0; side < 2; ++side) {
+        const uint32_t a = side ? (K - 1 - i) : i;
+        const uint32_t m0 = side ? (K - i) : (i + 1);
+        const __half* qa = data + (size_t)nei0[a] * dim;
+        for (uint32_t m = m0; m < K; m += 4) {
+          uint32_t ids[4];
+          float r4[4];
+#pragma unroll
+          for (int t = 0; t < 4; ++t) ids[t] = (m + t < K) ? nei0[m + t] : kInv;
+          warp_dist4(qa, data, dim, ids, r4, lane);
+          if (lane == 0) {
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+              if (m + t < K && r4[t] < nrow[m + t]) det[m + t] += 1;
+          }
+          __syncwarp();
+        }
+      }
+    }
+    warp_network(K, lane, [&](uint32_t u, uint32_t v) { return det[u] > det[v]; },
+                 [&](uint32_t u, uint32_t v) {
+                   swap_(det[u], det[v]);
+                   swap_(nei0[u], nei0[v]);
+                 });
+    for (uint32_t i = lane; i < d; i += 32) {
+      E_tgt[(size_t)b * d + i] = nei0[i];
+      E_val[(size_t)b * d + i] = det[i];
+      hybrid[(size_t)b * K + i] = nei0[i];
+    }
+    __syncwarp();
+  }
+}
+
+// filter_reverse_1hop (:1812-1886): dense stride-d rows written over the
+// graph buffer (no kernel of this stage reads it), first d/2 forward,
+// then reverse ids by ascending detour that are not already forward, then the
+// remaining forward ids.
+__global__ void __launch_bounds__(kWarps * 32)
+    k_filter_reverse_1hop(uint32_t* __restrict__ out, const uint32_t* __restrict__ rg,
+                          const uint32_t* __restrict__ rnum, const uint32_t* __restrict__ hybrid,
+                          uint32_t n, uint32_t K, uint32_t d) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned char* mine = smem + (size_t)warp * ((size_t)d * 16);
+  uint32_t* rev = reinterpret_cast<uint32_t*>(mine);
+  uint32_t* rdet = rev + d;
+  uint32_t* nid = rdet + d;
+  uint32_t* row = nid + d;
+  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+    const uint32_t rn = min(d, rnum[b]);
+    for (uint32_t i = lane; i < rn; i += 32) {
+      rev[i] = rg[(size_t)b * d * 2 + i * 2];
+      rdet[i] = rg[(size_t)b * d * 2 + i * 2 + 1];
+    }
+    for (uint32_t i = lane; i < d; i += 32) nid[i] = hybrid[(size_t)b * K + i];
+    __syncwarp();
+    warp_network(rn, lane, [&](uint32_t u, uint32_t v) { return rev[u] > rev[v]; },
+                 [&](uint32_t u, uint32_t v) {
+                   swap_(rev[u], rev[v]);
+                   swap_(rdet[u], rdet[v]);
+                 });
+    {
+      unsigned marks[4];
+      for (uint32_t c = 0; c * 32 < rn; ++c) {
+        const uint32_t i = c * 32 + lane;
+        marks[c] = __ballot_sync(kFull, i >= 1 && i < rn && rev[i] == rev[i - 1]);
+      }
+      __syncwarp();
+      for (uint32_t c = 0; c * 32 < rn; ++c)
+        if ((marks[c] >> lane) & 1u) rdet[c * 32 + lane] = kInv;
+      __syncwarp();
+    }
+    for (uint32_t i = lane; i < d / 2; i += 32) row[i] = nid[i];
+    warp_network(rn, lane, [&](uint32_t u, uint32_t v) { return rdet[u] > rdet[v]; },
+                 [&](uint32_t u, uint32_t v) {
+                   swap_(rdet[u], rdet[v]);
+                   swap_(rev[u], rev[v]);
+                 });
+    uint32_t cnt = 0;
+    const uint32_t span = (rn < d / 2) ? (d - rn) : (d / 2);
+    for (uint32_t i = 0; i < rn; ++i) {
+      if (rn >= d / 2 && cnt >= d / 2) break;
+      const uint32_t r = rev[i];
+      bool flag = false;
+      for (uint32_t j0 = 0; j0 < span; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        if (__any_sync(kFull, j < span && nid[j] == r)) {
+          flag = true;
+          break;
+        }
+      }
+      if (!flag) {
+        if (lane == 0) row[d / 2 + cnt] = r;
+        ++cnt;
+      }
+    }
+    __syncwarp();
+    const uint32_t m = min(cnt, d / 2);
+    for (uint32_t i = lane; i < d / 2 - m; i += 32) row[d / 2 + m + i] = nid[i + d / 2];
+    __syncwarp();
+    const uint32_t written = 2 * (d / 2);
+    for (uint32_t i = lane; i < written; i += 32) out[(size_t)b * d + i] = row[i];
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic reverse-edge store. Edges e = src * stride + i are sorted by
+// target with a stable radix sort, so each target's edges come in ascending
+// (source, i). Slot s of a target then receives, in that order, the inserts
+// whose running count c satisfies c == s (direct, c < cap) or c % mod == s
+// (replacement, c >= cap), as in the sequential reading of :1465-1475 and
+// :1697-1707.
+__global__ void k_edge_keys(const uint32_t* __restrict__ E_tgt, const uint32_t* __restrict__ cnt,
+                            uint32_t n, uint32_t stride, uint32_t* __restrict__ keys,
+                            uint32_t* __restrict__ vals, uint32_t* __restrict__ deg) {
+  const size_t total = (size_t)n * stride;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t src = (uint32_t)(e / stride), i = (uint32_t)(e % stride);
+    const bool valid = cnt ? (i < cnt[src]) : true;
+    const uint32_t t = valid ? E_tgt[e] : n;
+    keys[e] = t;
+    vals[e] = (uint32_t)e;
+    if (valid) atomicAdd(&deg[t], 1u);
+  }
+}
+
+// mode 0: (id, f32 dist) into rg[t*K+s], rd[t*128+s], replace when closer.
+// mode 1: (id, u32 detour) pairs into rg[t*2d + 2s], replace when fewer detours.
+template <int kMode>
+__global__ void k_reverse_fill(const uint32_t* __restrict__ sorted_e,
+                               const uint32_t* __restrict__ deg, const uint32_t* __restrict__ off,
+                               const uint32_t* __restrict__ E_val, uint32_t n, uint32_t stride,
+                               uint32_t cap, uint32_t mod, uint32_t K, uint32_t* __restrict__ rg,
+                               float* __restrict__ rd, uint32_t* __restrict__ rnum) {
+  const int lane = threadIdx.x & 31;
+  for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n;
+       t += (gridDim.x * blockDim.x) >> 5) {
+    const uint32_t c0 = rnum[t], dg = deg[t], o = off[t];
+    for (uint32_t s = lane; s < mod; s += 32) {
+      uint32_t cur_id, cur_v;
+      if (kMode == 0) {
+        cur_id = rg[(size_t)t * K + s];
+        cur_v = __float_as_uint(rd[(size_t)t * kReserve + s]);
+      } else {
+        cur_id = rg[(size_t)t * mod * 2 + 2 * s];
+        cur_v = rg[(size_t)t * mod * 2 + 2 * s + 1];
+      }
+      bool touched = false;
+      // smallest c >= c0 with c % mod == s
+      uint32_t c = (c0 <= s) ? s : (s + ((c0 - s + mod - 1) / mod) * mod);
+      for (; c < c0 + dg; c += mod) {
+        const uint32_t e = sorted_e[o + (c - c0)];
+        const uint32_t src = e / stride, v = E_val[e];
+        bool take;
+        if (c < cap) take = true;
+        else if (kMode == 0) take = __uint_as_float(v) < __uint_as_float(cur_v);
+        else take = cur_v > v;
+        if (take) {
+          cur_id = src;
+          cur_v = v;
+          touched = true;
+        }
+      }
+      if (touched) {
+        if (kMode == 0) {
+          rg[(size_t)t * K + s] = cur_id;
+          rd[(size_t)t * kReserve + s] = __uint_as_float(cur_v);
+        } else {
+          rg[(size_t)t * mod * 2 + 2 * s] = cur_id;
+          rg[(size_t)t * mod * 2 + 2 * s + 1] = cur_v;
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0) rnum[t] = c0 + dg;
+  }
+}
+
+int grid_for(uint32_t items_per_block, uint64_t items) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const uint64_t need = (items + items_per_block - 1) / items_per_block;
+  const uint64_t cap = (uint64_t)sms * 16;
+  return (int)std::max<uint64_t>(1, std::min<uint64_t>(need, cap));
+}
+
+int reverse_store(const Dev& d, const uint32_t* E_tgt, const uint32_t* E_val, const uint32_t* cnt,
+                  uint32_t stride, int mode, uint32_t cap, uint32_t mod, cudaStream_t s) {
+  const size_t E = (size_t)d.n * stride;
+  if (E >= 0xFFFFFFFFull) return fail(TAGORE_EINVAL, "too many reverse edges (%zu)", E);
+  int end_bit = 1;
+  while (end_bit < 32 && ((uint64_t)1 << end_bit) <= d.n) ++end_bit;
+  size_t sort_tmp = 0, scan_tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (uint32_t*)nullptr, (uint32_t*)nullptr, (int)E, 0, end_bit, s);
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                (int)d.n, s);
+  const size_t tmp = std::max(sort_tmp, scan_tmp);
+  Scratch sc(s);
+  const size_t bytes = E * 16 + (size_t)d.n * 8 + tmp + 256;
+  TG_TRY(sc.alloc(bytes));
+  uint32_t* keys = sc.as<uint32_t>();
+  uint32_t* vals = keys + E;
+  uint32_t* keys2 = vals + E;
+  uint32_t* vals2 = keys2 + E;
+  uint32_t* deg = vals2 + E;
+  uint32_t* off = deg + d.n;
+  void* tmp_p = reinterpret_cast<void*>(((uintptr_t)(off + d.n) + 255) & ~(uintptr_t)255);
+  TG_CUDA(cudaMemsetAsync(deg, 0, (size_t)d.n * 4, s));
+  k_edge_keys<<<grid_for(256, E), 256, 0, s>>>(E_tgt, cnt, d.n, stride, keys, vals, deg);
+  TG_CUDA(cudaGetLastError());
+  size_t t1 = tmp;
+  TG_CUDA(cub::DeviceScan::ExclusiveSum(tmp_p, t1, deg, off, (int)d.n, s));
+  t1 = tmp;
+  TG_CUDA(cub::DeviceRadixSort::SortPairs(tmp_p, t1, keys, keys2, vals, vals2, (int)E, 0, end_bit,
+                                          s));
+  const int grid = grid_for(8, d.n);
+  if (mode == 0)
+    k_reverse_fill<0><<<grid, 256, 0, s>>>(vals2, deg, off, E_val, d.n, stride, cap, mod, d.k,
+                                           d.rgraph, d.rd, d.rnum);
+  else
+    k_reverse_fill<1><<<grid, 256, 0, s>>>(vals2, deg, off, E_val, d.n, stride, cap, mod, d.k,
+                                           d.rgraph, d.rd, d.rnum);
+  TG_CUDA(cudaGetLastError());
+  return TAGORE_OK;
+}
+
+int validate(const Dev& d, cudaStream_t s) {
+  Scratch sc(s);
+  TG_TRY(sc.alloc(4));
+  TG_CUDA(cudaMemsetAsync(sc.p, 0, 4, s));
+  const size_t cnt = (size_t)d.n * d.k;
+  k_validate<<<grid_for(256, cnt), 256, 0, s>>>(d.graph, cnt, d.n, sc.as<uint32_t>());
+  TG_CUDA(cudaGetLastError());
+  uint32_t bad = 0;
+  TG_CUDA(cudaMemcpyAsync(&bad, sc.p, 4, cudaMemcpyDeviceToHost, s));
+  TG_CUDA(cudaStreamSynchronize(s));
+  if (bad) return fail(TAGORE_EINVAL, "graph holds an id >= POINTS (%u)", d.n);
+  return TAGORE_OK;
+}
+
+int check_shape(const Dev& d, uint32_t fd) {
+  if (d.n == 0 || d.k == 0 || d.dim == 0) return fail(TAGORE_EINVAL, "empty graph");
+  if (d.dim % 4) return fail(TAGORE_EINVAL, "DIM must be a multiple of 4 (got %u)", d.dim);
+  if (d.k > 128) return fail(TAGORE_EINVAL, "K must be <= 128 (got %u)", d.k);
+  if (fd == 0 || fd > d.k) return fail(TAGORE_EINVAL, "FINAL_DEGREE must be in [1, K]");
+  return TAGORE_OK;
+}
+
+int set_smem(const void* fn, size_t bytes) {
+  if (bytes > 227 * 1024) return fail(TAGORE_EINVAL, "shared memory request too large (%zu)", bytes);
+  TG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return TAGORE_OK;
+}
+
+// Select (path or 2-hop) + reverse store + filter_reverse.
+int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint32_t* ep_host,
+                   cudaStream_t s) {
+  const uint32_t fd = a.final_degree, K = d.k;
+  if (!path && K * K < kSelectCand) return fail(TAGORE_EINVAL, "2-hop collect needs K*K >= 480");
+  if (path && a.topm == 0) return fail(TAGORE_EINVAL, "TOPM must be >= 1");
+  Scratch sc(s);
+  TG_TRY(sc.alloc((size_t)d.n * fd * 8 + (size_t)d.n * 4 + 16));
+  uint32_t* P_ids = sc.as<uint32_t>();
+  float* P_dis = reinterpret_cast<float*>(P_ids + (size_t)d.n * fd);
+  uint32_t* P_cnt = reinterpret_cast<uint32_t*>(P_dis + (size_t)d.n * fd);
+  uint32_t* ep_dev = P_cnt + d.n;
+  if (path) {
+    const uint32_t W = a.topm + K;
+    const size_t sm = (size_t)W * 12 + ((W + 15u) & ~15u) + 64;
+    TG_TRY(set_smem((const void*)k_cal_ep, sm));
+    k_cal_ep<<<1, 32, sm, s>>>(d.graph, d.data, d.center, d.dim, K, a.topm, ep_dev);
+    TG_CUDA(cudaGetLastError());
+  }
+  SelLayout lay{path ? a.topm + K : 0u, kSelectCand + K, fd};
+  const size_t sm = lay.bytes() * kWarps;
+  const void* fn = path ? (const void*)k_select<true> : (const void*)k_select<false>;
+  TG_TRY(set_smem(fn, sm));
+  const int grid = grid_for(kWarps, d.n);
+  if (path)
+    k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
+                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+  else
+    k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
+                                                  a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+  TG_CUDA(cudaGetLastError());
+  TG_TRY(reverse_store(d, P_ids, reinterpret_cast<const uint32_t*>(P_dis), P_cnt, fd, 0, K, K, s));
+  const size_t sm2 = ((size_t)(fd + K) * 8 + (size_t)fd * 8 + 16) * kWarps;
+  TG_TRY(set_smem((const void*)k_filter_reverse, sm2));
+  k_filter_reverse<<<grid, kWarps * 32, sm2, s>>>(d.graph, d.nd, d.rgraph, d.rd, d.rnum, d.data,
+                                                  d.n, d.dim, K, fd, metric, a.thre, P_ids, P_cnt);
+  TG_CUDA(cudaGetLastError());
+  if (path && ep_host) {
+    TG_CUDA(cudaMemcpyAsync(ep_host, ep_dev, 4, cudaMemcpyDeviceToHost, s));
+  }
+  TG_CUDA(cudaStreamSynchronize(s));
+  return TAGORE_OK;
+}
+
+int run_rank_prune(const Dev& d, const PruneArgs& a, bool dpg, cudaStream_t s) {
+  const uint32_t K = d.k, dd = a.final_degree;
+  if (2 * dd > kReserve) return fail(TAGORE_EINVAL, "degree must be <= 64 for rank prunes");
+  uint32_t cap = dd;
+  if (dpg) {
+    if (K < dd + 1 || K - dd - 1 > dd)
+      return fail(TAGORE_EINVAL,
+                  "DPG needs degree+1 <= K <= 2*degree+1 (the reference's reverse rows overflow)");
+    cap = K - dd - 1;
+  }
+  Scratch sc(s);
+  TG_TRY(sc.alloc((size_t)d.n * dd * 8 + 16));
+  uint32_t* E_tgt = sc.as<uint32_t>();
+  uint32_t* E_val = E_tgt + (size_t)d.n * dd;
+  const int grid = grid_for(kWarps, d.n);
+  if (!dpg) {
+    const size_t sm = (256 * 4 + (size_t)K * 8) * kWarps;
+    TG_TRY(set_smem((const void*)k_select_cagra, sm));
+    k_select_cagra<<<grid, kWarps * 32, sm, s>>>(d.graph, d.n, K, dd, d.hybrid, E_tgt, E_val);
+  } else {
+    const size_t sm = ((size_t)K * 12) * kWarps;
+    TG_TRY(set_smem((const void*)k_select_dpg, sm));
+    k_select_dpg<<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, dd, d.hybrid,
+                                               E_tgt, E_val);
+  }
+  TG_CUDA(cudaGetLastError());
+  TG_TRY(reverse_store(d, E_tgt, E_val, nullptr, dd, 1, cap, dd, s));
+  const size_t sm2 = ((size_t)dd * 16) * kWarps;
+  TG_TRY(set_smem((const void*)k_filter_reverse_1hop, sm2));
+  k_filter_reverse_1hop<<<grid, kWarps * 32, sm2, s>>>(d.graph, d.rgraph, d.rnum, d.hybrid, d.n,
+                                                       K, dd);
+  TG_CUDA(cudaGetLastError());
+  TG_CUDA(cudaStreamSynchronize(s));
+  return TAGORE_OK;
+}
+
+}  // namespace
+
+int stage_cal_ep(const Dev& d, uint32_t topm, uint32_t* ep_host, cudaStream_t s) {
+  TG_TRY(check_shape(d, 1));
+  TG_TRY(validate(d, s));
+  Scratch sc(s);
+  TG_TRY(sc.alloc(4));
+  const uint32_t W = topm + d.k;
+  const size_t sm = (size_t)W * 12 + ((W + 15u) & ~15u) + 64;
+  TG_TRY(set_smem((const void*)k_cal_ep, sm));
+  k_cal_ep<<<1, 32, sm, s>>>(d.graph, d.data, d.center, d.dim, d.k, topm, sc.as<uint32_t>());
+  TG_CUDA(cudaGetLastError());
+  TG_CUDA(cudaMemcpyAsync(ep_host, sc.p, 4, cudaMemcpyDeviceToHost, s));
+  TG_CUDA(cudaStreamSynchronize(s));
+  return TAGORE_OK;
+}
+
+int prune_index(const Dev& d, const PruneArgs& a, const std::string& type, uint32_t* ep_host,
+                cudaStream_t s) {
+  TG_TRY(check_shape(d, a.final_degree));
+  TG_TRY(validate(d, s));
+  if (type == "NSG" || type == "Vamana") {
+    PruneArgs b = a;
+    if (type == "NSG") b.thre = 1.0f;  // pybind.cu:181,183 pass 1.0
+    return run_dist_prune(d, b, true, 0, ep_host, s);
+  }
+  if (type == "NSSG") return run_dist_prune(d, a, false, 1, ep_host, s);
+  if (type == "CAGRA") return run_rank_prune(d, a, false, s);
+  if (type == "DPG") return run_rank_prune(d, a, true, s);
+  return fail(TAGORE_EINVAL, "unknown index_type '%s' (NSG, Vamana, NSSG, CAGRA, DPG)",
+              type.c_str());
+}
+
+int prune_cfs(const Dev& d, const PruneArgs& a, const std::string& mode, const std::string& metric,
+              uint32_t* ep_host, cudaStream_t s) {
+  TG_TRY(check_shape(d, a.final_degree));
+  TG_TRY(validate(d, s));
+  const bool dist_like = metric == "dist" || metric == "angle";
+  const int m = metric == "angle" ? 1 : 0;
+  if (mode == "path" && dist_like) return run_dist_prune(d, a, true, m, ep_host, s);
+  if (mode == "2-hop" && dist_like) return run_dist_prune(d, a, false, m, ep_host, s);
+  if (mode == "1-hop" && metric == "rank") return run_rank_prune(d, a, false, s);
+  return fail(TAGORE_EINVAL,
+              "unsupported CFS combination mode='%s' metric='%s' (path|2-hop with dist|angle, "
+              "1-hop with rank)",
+              mode.c_str(), metric.c_str());
+}
+
+}  // namespace tagore
