@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Index-build benchmark: 1M x 128 (SIFT-like mixture), GNN-Descent k=96 with
+10 iterations, then the CFS 'path'/'dist' prune (NSG rule) to degree 32, m=64.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step builds the whole index once. `value` is seconds per build with the
+FP32 base already resident in HBM (timed with CUDA events on the stream the
+library launches on, max over ranks); `e2e` is the same build through the C
+ABI from host memory to host memory (H2D of the base and D2H of the pruned
+rows inside the timed region). Under torchrun every rank builds its own
+replica (weak scaling). `--impl reference` times the CPU implementation of the
+path (the oracle port: OpenMP NN-Descent + path prune) on a bounded sample.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "1M×128 index build s (GNN-Descent+prune), chosen vs plain FP32 @ equal recall"
+K, ITERS, FD, TOPM, THRE = 96, 10, 32, 64, 1.0
+
+
+def args_():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--cpu-sample", type=int, default=40_000)
+    ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-recall", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """Samples SM clock and throttle reasons every 200 ms (read-only NVML)."""
+
+    BITS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+            0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, index):
+        self.samples, self.reasons, self.stop_ev = [], set(), threading.Event()
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                r = self.nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.BITS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self.stop_ev.wait(0.2)
+
+    def __enter__(self):
+        if self.nv:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        if self.nv:
+            self.stop_ev.set()
+            self.t.join()
+
+    def summary(self):
+        med = statistics.median(self.samples) if self.samples else None
+        return {"sm_mhz": med, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                "samples": len(self.samples)}
+
+
+def stage_stats(capi):
+    L = capi.lib()
+    arr = (capi.StageStat * 32)()
+    cnt = C.c_int(0)
+    capi.check(L.tagore_stage_stats(arr, 32, C.byref(cnt)))
+    return {arr[i].name.decode(): (arr[i].ms, arr[i].launches, arr[i].bytes, arr[i].items)
+            for i in range(min(cnt.value, 32))}
+
+
+def recall_knn(g, half_t, samp, k=10):
+    import torch
+    x = half_t.float()
+    q = x[samp]
+    d2 = (q * q).sum(1, keepdim=True) + (x * x).sum(1)[None] - 2.0 * (q @ x.T)
+    d2[torch.arange(len(samp)), torch.as_tensor(samp, device=x.device)] = float("inf")
+    truth = torch.topk(d2, k, largest=False).indices.cpu().numpy()
+    return float(np.mean([len(set(g[s, :k].tolist()) & set(truth[i].tolist())) / k
+                          for i, s in enumerate(samp)]))
+
+
+def index_recall(rows, ep, base, queries, half_t, k=10, L=64):
+    """recall@10 of a fixed greedy search (pool L) over the pruned rows."""
+    import torch
+    from oracle import oracle as orc
+    n = rows.shape[0]
+    deg = rows[:, 0].astype(np.int64)
+    offs = np.zeros(n + 1, np.uint64)
+    offs[1:] = np.cumsum(deg)
+    mask = np.arange(rows.shape[1] - 1)[None, :] < deg[:, None]
+    adj = rows[:, 1:][mask].astype(np.uint32)
+    x = base.astype(np.float32)
+    found = orc.greedy_search(x, offs, adj, ep, queries, L, k)
+    xq = torch.as_tensor(queries, device=half_t.device)
+    xb = torch.as_tensor(x, device=half_t.device)
+    d2 = (xq * xq).sum(1, keepdim=True) + (xb * xb).sum(1)[None] - 2.0 * (xq @ xb.T)
+    truth = torch.topk(d2, k, largest=False).indices.cpu().numpy()
+    return float(np.mean([len(set(found[i].tolist()) & set(truth[i].tolist())) / k
+                          for i in range(len(queries))]))
+
+
+def cpu_baseline(base, n_total, sample):
+    """Oracle port (OpenMP NN-Descent + path prune) on the first `sample`
+    points; seconds scaled to the full base by n_total / sample."""
+    from oracle import oracle as orc
+    xs = np.ascontiguousarray(base[:sample])
+    half, center, factor = orc.host_prep(xs)
+    t0 = time.perf_counter()
+    ids, _ = orc.nndescent(half.astype(np.float32), K, ITERS)
+    dis = orc.dist_pairs(half, np.repeat(np.arange(sample, dtype=np.uint32), K), ids.reshape(-1))
+    dis = dis.reshape(sample, K)
+    order = np.argsort(dis, axis=1, kind="stable")
+    buf = orc.Buffers(np.take_along_axis(ids, order, 1), np.take_along_axis(dis, order, 1), half,
+                      center)
+    orc.prune_cfs(buf, FD, "path", "dist", topm=TOPM, thre=THRE)
+    sec = time.perf_counter() - t0
+    return {"value": sec * n_total / sample, "unit": "s", "cores": orc.num_threads(),
+            "kind": "port",
+            "sample": f"first {sample} of the {n_total} base vectors, same K/iterations/prune; "
+                      f"{sec:.2f}s measured, scaled by {n_total}/{sample}"}
+
+
+def reference_arm(a, rank):
+    if rank != 0:
+        return
+    from tagore_b200 import synth
+    base, _ = synth.config(1, n=a.n)
+    sample = min(a.cpu_sample, a.n)
+    for _ in range(a.warmup):
+        cpu_baseline(base, a.n, max(2000, sample // 8))
+    vals = []
+    for _ in range(a.steps):
+        vals.append(cpu_baseline(base, a.n, sample))
+    v = statistics.mean(x["value"] for x in vals)
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": a.gpus,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": v * 1000.0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic SIFT-like mixture (seeded), bounded CPU sample",
+            "config": {"workload": "1M x 128 SIFT-like, GNN-Descent k=96 x10 + CFS path/dist "
+                                   "1.0 degree 32 m=64", "n": a.n, "dim": 128, "k": K,
+                       "iters": ITERS, "final_degree": FD, "topm": TOPM},
+            "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = args_()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        reference_arm(a, rank)
+        return
+    import torch
+    from tagore_b200 import capi, synth
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    L = capi.lib()
+    base, queries = synth.config(1, n=a.n, nq=1000)
+    n, dim = base.shape
+    dev = torch.from_numpy(base).cuda()
+    stream = torch.cuda.current_stream()
+    capi.check(L.tagore_set_stream(C.c_void_p(stream.cuda_stream)))
+
+    def build(mode):
+        p = capi.knn_params(K, n, dim, ITERS, mode)
+        st = capi.State()
+        capi.check(L.tagore_gnn_descent_device(C.byref(p), C.c_void_p(dev.data_ptr()),
+                                               base.ctypes.data_as(C.c_void_p), n, dim,
+                                               C.byref(st.st)))
+        capi.pruning_cfs(st, FD, "path", "dist", topm=TOPM, thre=THRE)
+        return st
+
+    def timed(mode, steps, warmup):
+        for _ in range(warmup):
+            build(mode).free()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        capi.check(L.tagore_reset_counters())
+        capi.check(L.tagore_set_profiling(1))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            e0.record(stream)
+            for _ in range(steps):
+                build(mode).free()
+            e1.record(stream)
+            torch.cuda.synchronize()
+        capi.check(L.tagore_set_profiling(0))
+        ms = e0.elapsed_time(e1) / steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        launches = capi.last_timings().kernel_launches
+        return ms, stage_stats(capi), launches, clk.summary()
+
+    ms, stages, launches, clocks = timed(capi.KNN_CHOSEN, a.steps, a.warmup)
+    plain_ms = None
+    if not a.skip_plain:
+        plain_ms, _, _, _ = timed(capi.KNN_PLAIN, max(1, a.steps // 2), 1)
+
+    # dominant stage -> roofline (algorithmic bytes per launch / mean launch time)
+    name, (s_ms, s_launch, s_bytes, s_items) = max(stages.items(), key=lambda kv: kv[1][0])
+    peak, peak_kind = peaks()
+    achieved = (s_bytes / max(1, s_launch)) / ((s_ms / max(1, s_launch)) * 1e-3) / 1e9 if s_bytes else None
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(name)
+
+    extra = {}
+    if not a.skip_recall and rank == 0:
+        samp = np.random.default_rng(0).choice(n, 1000, replace=False)
+        for label, mode in (("chosen", capi.KNN_CHOSEN), ("plain", capi.KNN_PLAIN)):
+            if label == "plain" and a.skip_plain:
+                continue
+            p = capi.knn_params(K, n, dim, ITERS, mode)
+            st = capi.State()
+            capi.check(L.tagore_gnn_descent_device(C.byref(p), C.c_void_p(dev.data_ptr()),
+                                                   base.ctypes.data_as(C.c_void_p), n, dim,
+                                                   C.byref(st.st)))
+            g = st.download(0).reshape(n, K)
+            half_t = torch.from_numpy(st.download(2).reshape(n, dim)).cuda()
+            extra[f"knn_recall10_{label}"] = recall_knn(g, half_t, samp)
+            ep = capi.pruning_cfs(st, FD, "path", "dist", topm=TOPM, thre=THRE)
+            rows = st.download(0).reshape(n, K)
+            extra[f"index_recall10_{label}"] = index_recall(rows, ep, base, queries, half_t)
+            st.free()
+
+    e2e = None
+    if not a.skip_e2e:
+        capi.check(L.tagore_set_stream(None))
+        out = np.empty((n, K), np.uint32)
+        capi.build_index_host(base, K, ITERS, FD, TOPM, THRE, out=out)
+        ts = []
+        for _ in range(a.steps):
+            t0 = time.perf_counter()
+            capi.build_index_host(base, K, ITERS, FD, TOPM, THRE, out=out)
+            ts.append(time.perf_counter() - t0)
+        e2e_s = statistics.mean(ts)
+        if dist:
+            t = torch.tensor([e2e_s], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(base.nbytes),
+               "d2h_bytes_per_step": int(out.nbytes)}
+
+    cpu = None
+    if not a.skip_cpu and rank == 0 and world == 1:
+        cpu = cpu_baseline(base, n, min(a.cpu_sample, n))
+
+    if rank == 0:
+        value = ms / 1000.0
+        line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f16 storage, f32 arithmetic (tcgen05 f16 screen)",
+                "data": "synthetic SIFT-like mixture (seeded, 256 components)",
+                "config": {"workload": "1M x 128 SIFT-like, GNN-Descent k=96 x10 + CFS path/dist "
+                                       "1.0 degree 32 m=64", "n": n, "dim": dim, "k": K,
+                           "iters": ITERS, "final_degree": FD, "topm": TOPM,
+                           "l2": "inputs larger than L2 (512 MB FP32 + 256 MB FP16 base)",
+                           "parallelism": f"replicas x{world}"},
+                "vectors_per_s": world * n / value,
+                "plain_fp32_s": plain_ms / 1000.0 if plain_ms else None,
+                "chosen_speedup_vs_plain": (plain_ms / ms) if plain_ms else None,
+                "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                             "peak_source": peak_kind, "traffic": traffic,
+                             "algorithmic_bytes_per_launch": s_bytes / max(1, s_launch),
+                             "ms_per_launch": s_ms / max(1, s_launch)},
+                "stages_ms_per_step": {k: v[0] / a.steps for k, v in stages.items()},
+                "gpu_launches": launches,
+                "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    capi.check(L.tagore_set_stream(None))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

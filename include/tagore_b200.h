@@ -148,12 +148,40 @@ int tagore_store_cagra(const char* path, const uint32_t* graph, uint32_t n, uint
 int tagore_load_fvecs_header(const char* path, uint32_t* n, uint32_t* dim);
 int tagore_load_fvecs(const char* path, float* out, uint32_t n, uint32_t dim);
 
-/* Timings of the last build on this thread (milliseconds). */
+/* Same as tagore_gnn_descent_host with the FP32 base already on the current
+ * device (dev_data). host_data is the same base in host memory: the
+ * power-of-ten factor and the centroid are computed from it on host threads,
+ * in the reference's order, while the device builds the graph. */
+int tagore_gnn_descent_device(const TagoreKnnParams* p, const float* dev_data,
+                              const float* host_data, uint32_t n, uint32_t dim,
+                              TagoreKnnState* out);
+
+/* Work of later calls on this thread goes to `stream` (a cudaStream_t; NULL
+ * restores a private stream per call). Calls still return only when their
+ * work has finished. */
+int tagore_set_stream(void* stream);
+
+/* Timings of the last build on this thread (milliseconds) and the number of
+ * kernels this library launched since the last tagore_reset_counters(). */
 typedef struct TagoreTimings {
   double knn_ms, prune_ms, prep_ms, total_ms;
   uint64_t kernel_launches;
 } TagoreTimings;
 int tagore_last_timings(TagoreTimings* t);
+int tagore_reset_counters(void);
+
+/* Per-stage device timing, recorded with CUDA events around each launch on
+ * the launching stream while profiling is on. bytes is the stage's
+ * algorithmic traffic (rows gathered x row bytes, list and pool traffic). */
+typedef struct TagoreStageStat {
+  char name[32];
+  double ms;
+  uint64_t launches;
+  uint64_t bytes;
+  uint64_t items;
+} TagoreStageStat;
+int tagore_set_profiling(int on);
+int tagore_stage_stats(TagoreStageStat* out, int max, int* count);
 
 /* Frees a device buffer this library allocated (capsule destructor). */
 int tagore_device_free(void* p);

@@ -56,6 +56,11 @@ class Timings(C.Structure):
                 ("total_ms", C.c_double), ("kernel_launches", C.c_uint64)]
 
 
+class StageStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("ms", C.c_double), ("launches", C.c_uint64),
+                ("bytes", C.c_uint64), ("items", C.c_uint64)]
+
+
 # Every exported entry point with its C signature (restype, argtypes).
 SIGNATURES = {
     "tagore_gnn_descent": (C.c_int, [C.POINTER(KnnParams), C.c_char_p, C.POINTER(KnnState)]),
@@ -87,6 +92,12 @@ SIGNATURES = {
                                            C.POINTER(C.c_uint32)]),
     "tagore_load_fvecs": (C.c_int, [C.c_char_p, C.c_void_p, C.c_uint32, C.c_uint32]),
     "tagore_last_timings": (C.c_int, [C.POINTER(Timings)]),
+    "tagore_gnn_descent_device": (C.c_int, [C.POINTER(KnnParams), C.c_void_p, C.c_void_p,
+                                            C.c_uint32, C.c_uint32, C.POINTER(KnnState)]),
+    "tagore_set_stream": (C.c_int, [C.c_void_p]),
+    "tagore_reset_counters": (C.c_int, []),
+    "tagore_set_profiling": (C.c_int, [C.c_int]),
+    "tagore_stage_stats": (C.c_int, [C.POINTER(StageStat), C.c_int, C.POINTER(C.c_int)]),
     "tagore_device_free": (C.c_int, [C.c_void_p]),
     "tagore_last_error": (C.c_char_p, []),
     "tagore_version": (C.c_char_p, []),

@@ -1,5 +1,6 @@
 // capi.cu -- the C ABI (include/tagore_b200.h): argument checks, buffer
 // ownership, streams, timings and error reporting around the kernel files.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -13,6 +14,75 @@ namespace tagore {
 
 static thread_local std::string g_err;
 static thread_local TagoreTimings g_times{};
+static thread_local cudaStream_t g_user_stream = nullptr;
+static std::atomic<uint64_t> g_launches{0};
+
+// ---- stage timing ----
+struct StageRec {
+  std::string name;
+  cudaEvent_t a = nullptr, b = nullptr;
+  bool closed = false;
+};
+static thread_local bool g_prof = false;
+static thread_local std::vector<StageRec> g_open;
+static thread_local std::vector<TagoreStageStat> g_stats;
+
+static TagoreStageStat& stat_of(const char* name) {
+  for (auto& s : g_stats)
+    if (std::strncmp(s.name, name, sizeof(s.name)) == 0) return s;
+  TagoreStageStat s{};
+  std::snprintf(s.name, sizeof(s.name), "%s", name);
+  g_stats.push_back(s);
+  return g_stats.back();
+}
+
+void count_launch(uint32_t n) { g_launches += n; }
+bool profiling() { return g_prof; }
+
+void stage_begin(const char* name, cudaStream_t s) {
+  if (!g_prof) return;
+  StageRec r;
+  r.name = name;
+  cudaEventCreate(&r.a);
+  cudaEventCreate(&r.b);
+  cudaEventRecord(r.a, s);
+  g_open.push_back(r);
+}
+
+void stage_end(const char* name, cudaStream_t s, uint64_t bytes, uint64_t items) {
+  if (!g_prof) return;
+  for (auto it = g_open.rbegin(); it != g_open.rend(); ++it)
+    if (!it->closed && it->name == name) {
+      cudaEventRecord(it->b, s);
+      it->closed = true;
+      break;
+    }
+  TagoreStageStat& st = stat_of(name);
+  st.launches += 1;
+  st.bytes += bytes;
+  st.items += items;
+}
+
+void stage_add(const char* name, uint64_t bytes, uint64_t items) {
+  if (!g_prof) return;
+  TagoreStageStat& st = stat_of(name);
+  st.bytes += bytes;
+  st.items += items;
+}
+
+// Resolves recorded events into milliseconds (the stream must be synchronised).
+static void stage_flush() {
+  for (auto& r : g_open) {
+    if (r.closed) {
+      float ms = 0.f;
+      cudaEventSynchronize(r.b);
+      if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) stat_of(r.name.c_str()).ms += ms;
+    }
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  g_open.clear();
+}
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -33,15 +103,26 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
 
 namespace {
 
-// A non-blocking stream owned by one API call.
+// The caller's stream (tagore_set_stream) or a non-blocking stream owned by
+// one API call.
 struct Stream {
   cudaStream_t s = nullptr;
+  bool own = false;
   int init() {
+    if (g_user_stream) {
+      s = g_user_stream;
+      return TAGORE_OK;
+    }
     TG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    own = true;
     return TAGORE_OK;
   }
   ~Stream() {
-    if (s) cudaStreamDestroy(s);
+    if (s) {
+      cudaStreamSynchronize(s);
+      stage_flush();
+    }
+    if (own) cudaStreamDestroy(s);
   }
 };
 
@@ -144,6 +225,32 @@ const char* tagore_version(void) { return "tagore_b200 0.1 (sm_100a)"; }
 int tagore_last_timings(TagoreTimings* t) {
   if (!t) return fail(TAGORE_EINVAL, "null timings");
   *t = g_times;
+  t->kernel_launches = g_launches.load();
+  return TAGORE_OK;
+}
+
+int tagore_reset_counters(void) {
+  g_launches = 0;
+  g_stats.clear();
+  return TAGORE_OK;
+}
+
+int tagore_set_stream(void* stream) {
+  g_user_stream = reinterpret_cast<cudaStream_t>(stream);
+  return TAGORE_OK;
+}
+
+int tagore_set_profiling(int on) {
+  g_prof = on != 0;
+  return TAGORE_OK;
+}
+
+int tagore_stage_stats(TagoreStageStat* out, int max, int* count) {
+  if (!count) return fail(TAGORE_EINVAL, "null count");
+  stage_flush();
+  const int n = (int)g_stats.size();
+  for (int i = 0; i < n && i < max && out; ++i) out[i] = g_stats[i];
+  *count = n;
   return TAGORE_OK;
 }
 
@@ -171,6 +278,7 @@ int tagore_state_alloc(uint32_t n, uint32_t dim, uint32_t k, TagoreKnnState* out
       return cuda_fail(e, "cudaMalloc(state)", __FILE__, __LINE__);
     }
   }
+  TG_CUDA(cudaDeviceSynchronize());  // zero fill done before work on any stream
   return TAGORE_OK;
 }
 
@@ -233,6 +341,21 @@ int tagore_gnn_descent_host(const TagoreKnnParams* p, const float* data, uint32_
   if (rc == TAGORE_OK) rc = build_from_device(p, raw, data, n, dim, out, st.s);
   cudaFreeAsync(raw, st.s);
   cudaStreamSynchronize(st.s);
+  if (rc != TAGORE_OK) tagore_state_free(out);
+  return rc;
+}
+
+int tagore_gnn_descent_device(const TagoreKnnParams* p, const float* dev_data,
+                              const float* host_data, uint32_t n, uint32_t dim,
+                              TagoreKnnState* out) {
+  if (!p || !dev_data || !host_data || !out) return fail(TAGORE_EINVAL, "null argument");
+  if (dim != p->dim) return fail(TAGORE_EINVAL, "DIM %u differs from the data's %u", p->dim, dim);
+  if (dim % 4) return fail(TAGORE_EINVAL, "DIM must be a multiple of 4 (got %u)", dim);
+  if (p->k == 0 || p->k >= n) return fail(TAGORE_EINVAL, "need POINTS > K >= 1");
+  Stream st;
+  TG_TRY(st.init());
+  TG_TRY(tagore_state_alloc(n, dim, p->k, out));
+  const int rc = build_from_device(p, dev_data, host_data, n, dim, out, st.s);
   if (rc != TAGORE_OK) tagore_state_free(out);
   return rc;
 }

@@ -26,6 +26,16 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
     if (rc_ != TAGORE_OK) return rc_; \
   } while (0)
 
+// ---- launch accounting and stage timing (capi.cu) ----
+void count_launch(uint32_t n = 1);
+bool profiling();
+// Records a start event for stage `name` on `s` (no-op when profiling is off);
+// stage_end records the stop event and the stage's algorithmic bytes/items.
+void stage_begin(const char* name, cudaStream_t s);
+void stage_end(const char* name, cudaStream_t s, uint64_t bytes = 0, uint64_t items = 0);
+// Adds bytes/items to a stage after the fact (counts read back from the device).
+void stage_add(const char* name, uint64_t bytes, uint64_t items);
+
 // Typed view of the eight reference buffers (capsule order, pybind.cu:132-141).
 struct Dev {
   uint32_t n, k, dim;

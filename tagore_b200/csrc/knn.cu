@@ -194,10 +194,11 @@ __global__ void __launch_bounds__(128)
   uint32_t* vec = reinterpret_cast<uint32_t*>(dm + kMaxList * (kMaxList + 1));
   const uint32_t tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  unsigned long long props = 0, pairs = 0;
+  unsigned long long props = 0, pairs = 0, rows = 0;
   for (uint32_t u = blockIdx.x; u < n; u += gridDim.x) {
     const uint32_t nn = lcnt[2 * u], total = lcnt[2 * u + 1];
     if (nn == 0 || total < 2) continue;
+    if (tid == 0) rows += total;
     if (tid < total) {
       list[tid] = lists[(size_t)u * kMaxList + tid];
       kth[tid] = kth_of(nb[(size_t)list[tid] * K + K - 1]);
@@ -246,6 +247,7 @@ __global__ void __launch_bounds__(128)
   }
   atomicAdd(&stats[0], props);
   atomicAdd(&stats[1], pairs);
+  if (tid == 0) atomicAdd(&stats[3], rows);
 }
 
 // Merges the pool of each node into its sorted row and clears the pool.
@@ -378,30 +380,51 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   TG_CUDA(cudaMemsetAsync(w.pool, 0xFF, poolB, s));
   TG_CUDA(cudaMemsetAsync(w.stats, 0, 64, s));
   const int sms = sm_count();
+  const uint64_t n64 = d.n;
+  stage_begin("knn_init", s);
   k_init<<<sms * 16, 128, 0, s>>>(d.data, d.n, d.dim, K, a.seed, w.nb);
+  count_launch();
+  stage_end("knn_init", s, n64 * K * (2ull * d.dim + 8), n64 * K);
   TG_CUDA(cudaGetLastError());
+  const char* join_name = a.mode == TAGORE_KNN_PLAIN ? "knn_join_plain" : "knn_join_tc";
   for (uint32_t it = 0; it < a.iters; ++it) {
     TG_CUDA(cudaMemsetAsync(w.rcnt, 0, (size_t)d.n * 8, s));
+    stage_begin("knn_sample", s);
     k_sample<<<sms * 16, 128, 0, s>>>(w.nb, d.n, K, S, w.fnew, w.fold, w.fcnt, w.rnew, w.rold,
                                        w.rcnt);
+    count_launch();
+    stage_end("knn_sample", s, n64 * K * 8 + n64 * 2 * S * 4 * 2, n64);
     TG_CUDA(cudaGetLastError());
+    stage_begin("knn_lists", s);
     k_build_lists<<<sms * 16, 128, 0, s>>>(d.n, S, w.fnew, w.fold, w.fcnt, w.rnew, w.rold, w.rcnt,
                                            w.lists, w.lcnt);
+    count_launch();
+    stage_end("knn_lists", s, n64 * 4 * S * 4 + n64 * kMaxList * 4, n64);
     TG_CUDA(cudaGetLastError());
+    stage_begin(join_name, s);
     if (a.mode == TAGORE_KNN_PLAIN) {
       TG_TRY(join_plain(w, s));
     } else {
       TG_TRY(join_tc(w, s));
     }
+    count_launch();
+    stage_end(join_name, s);
+    stage_begin("knn_merge", s);
     k_merge<<<sms * 16, 128, 0, s>>>(w.nb, w.pool, d.n, K, P, w.stats);
+    count_launch();
+    stage_end("knn_merge", s, n64 * (16ull * K + 16ull * P), n64);
     TG_CUDA(cudaGetLastError());
   }
   k_finalize<<<sms * 8, 256, 0, s>>>(w.nb, d.n, K, d.graph, d.nd);
+  count_launch();
   TG_CUDA(cudaGetLastError());
   unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   TG_CUDA(cudaMemcpyAsync(h, w.stats, sizeof(h), cudaMemcpyDeviceToHost, s));
   TG_CUDA(cudaStreamSynchronize(s));
   if ((uint32_t)h[4] != 0) return fail(TAGORE_ETIMEOUT, "tensor-core join: a bounded wait ran out");
+  // join traffic: each gathered row (FP16 vector, norm, k-th key, list id),
+  // one 8-byte count pair per node, one 8-byte read-modify-write per proposal
+  stage_add(join_name, h[3] * (2ull * d.dim + 16) + n64 * a.iters * 8 + h[0] * 16, h[1]);
   if (st) {
     st->proposals = h[0];
     st->pairs = h[1];

@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s.taddr;
   uint32_t phase = 0;
-  unsigned long long n_pairs = 0, n_props = 0;
+  unsigned long long n_pairs = 0, n_props = 0, n_rows = 0;
   bool failed = false;
 
   for (uint32_t u = blockIdx.x; u < n && !failed; u += gridDim.x) {
@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       __syncthreads();
       continue;
     }
+    if (tid == 0) n_rows += total;
     if (tid < total) {
       const uint32_t id = lists[(size_t)u * kMaxList + tid];
       s.ids[tid] = id;
@@ -285,6 +286,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     atomicAdd(&stats[0], n_props);
     atomicAdd(&stats[1], n_pairs);
   }
+  if (tid == 0) atomicAdd(&stats[3], n_rows);
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 0)
