@@ -1,6 +1,7 @@
 // capi.cu -- the C ABI (include/tagore_b200.h): argument checks, buffer
 // ownership, streams, timings and error reporting around the kernel files.
 #include <atomic>
+#include <chrono>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -203,9 +204,14 @@ int build_from_device(const TagoreKnnParams* p, const float* raw_dev, const floa
   std::thread cth(host_center, host_for_center, n, dim, st->norm_factor, center.data());
   KnnArgs a{p->k, p->iters, p->mode, p->sample, p->per_row, p->seed};
   KnnStats ks{};
+  const auto w0 = std::chrono::steady_clock::now();
   const int rc = knn_build(dev_of(st), (const float*)st->norms, a, &ks, s);
   g_times.knn_ms = t0.stop(s);
+  const auto w1 = std::chrono::steady_clock::now();
   cth.join();
+  const auto w2 = std::chrono::steady_clock::now();
+  g_times.prep_ms = std::chrono::duration<double, std::milli>(w2 - w1).count();  // centroid wait
+  g_times.total_ms = std::chrono::duration<double, std::milli>(w2 - w0).count();
   TG_TRY(rc);
   TG_CUDA(cudaMemcpyAsync(st->center, center.data(), (size_t)dim * 2, cudaMemcpyHostToDevice, s));
   TG_CUDA(cudaStreamSynchronize(s));
@@ -437,10 +443,49 @@ int tagore_build_index_host(const TagoreKnnParams* p, const float* data, uint32_
 }
 
 int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev) {
-  (void)p;
-  (void)devices;
-  (void)ndev;
-  return fail(TAGORE_EINVAL, "largeIndex is not available in this build");
+  if (!p || !devices) return fail(TAGORE_EINVAL, "null argument");
+  if (ndev == 1) TG_CUDA(cudaSetDevice((int)devices[0]));
+  // gpu_construct (src/large_index.cu:130-279) for one cluster: read
+  // [u32 n][n x dim f32], kNN graph without rescale, CFS path/dist prune with
+  // alpha = thre, rows back to the host with local ids mapped to global ones.
+  LargeBuildFn build = [](const TagoreLargeParams& q, uint32_t cid, const std::vector<uint32_t>& ids,
+                          std::vector<uint32_t>& rows, uint32_t* medoid) -> int {
+    const uint32_t n = (uint32_t)ids.size(), dim = q.dim;
+    const std::string path = std::string(q.data_prefix) + std::to_string(cid);
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) return fail(TAGORE_EIO, "cannot open cluster file '%s'", path.c_str());
+    uint32_t n_file = 0;
+    std::vector<float> x((size_t)n * dim);
+    const bool ok = std::fread(&n_file, 4, 1, f) == 1 && std::fread(x.data(), 4, x.size(), f) == x.size();
+    std::fclose(f);
+    if (!ok) return fail(TAGORE_EIO, "'%s' holds fewer than %u vectors", path.c_str(), n);
+    TagoreKnnParams kp{};
+    kp.k = q.k;
+    kp.n = n;
+    kp.dim = dim;
+    kp.iters = q.knn_iters ? q.knn_iters : 16;
+    kp.mode = q.mode;
+    kp.rescale = 0;
+    kp.seed = 0x7A6Eull + cid;
+    TagoreKnnState st{};
+    TG_TRY(tagore_gnn_descent_host(&kp, x.data(), n, dim, &st));
+    TagorePruneParams pp{q.k, n, dim, q.final_degree, q.topm, q.thre};
+    int rc = tagore_pruning_cfs(&pp, &st, "path", "dist");
+    if (rc == TAGORE_OK) {
+      rows.resize((size_t)n * q.k);
+      cudaError_t e = cudaMemcpy(rows.data(), st.graph, rows.size() * 4, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(cluster rows)", __FILE__, __LINE__);
+      *medoid = ids[st.ep];
+    }
+    tagore_state_free(&st);
+    TG_TRY(rc);
+    for (uint32_t i = 0; i < n; ++i) {
+      uint32_t* r = rows.data() + (size_t)i * q.k;
+      for (uint32_t j = 1; j <= r[0]; ++j) r[j] = ids[r[j]];
+    }
+    return TAGORE_OK;
+  };
+  return large_index_run(*p, devices, ndev, build);
 }
 
 }  // extern "C"

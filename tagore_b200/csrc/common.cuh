@@ -88,6 +88,42 @@ __device__ __forceinline__ void warp_dist4(const __half* __restrict__ q, const _
   for (int t = 0; t < 4; ++t) out[t] = __shfl_sync(kFull, __fadd_rn(x[t], y[t]), 0);
 }
 
+// The reference's shuffle-down tree evaluated by one thread over the 32 lane
+// slots: v_L[l] = v_{L-1}[l] + v_{L-1}[l + (32 >> L)], root v_5[0]. Walking
+// the tree depth-first visits the slots in bit-reversed order and keeps at
+// most five partial pairs alive. `leaf(slot, x, y)` accumulates that slot's
+// chunks (slot, slot + 32, ...) into (x, y) exactly as the lane would.
+template <int Level, int Slot, class Leaf>
+__device__ __forceinline__ void lane_tree(Leaf& leaf, float& x, float& y) {
+  if constexpr (Level == 0) {
+    x = 0.0f;
+    y = 0.0f;
+    leaf(Slot, x, y);
+  } else {
+    float ax, ay, bx, by;
+    lane_tree<Level - 1, Slot>(leaf, ax, ay);
+    lane_tree<Level - 1, Slot + (32 >> Level)>(leaf, bx, by);
+    x = __fadd_rn(ax, bx);
+    y = __fadd_rn(ay, by);
+  }
+}
+
+// Exact FP32 squared L2 in the reference's lane order by a single thread;
+// chunk(j) returns the two 4-half chunks j of the operands.
+template <int D, class Chunk>
+__device__ __forceinline__ float serial_dist(Chunk chunk) {
+  auto leaf = [&](int slot, float& x, float& y) {
+#pragma unroll
+    for (int j = slot; j < D / 4; j += 32) {
+      const uint2 a = chunk(j, 0), b = chunk(j, 1);
+      chunk_acc(a, b, x, y);
+    }
+  };
+  float x, y;
+  lane_tree<5, 0>(leaf, x, y);
+  return __fadd_rn(x, y);
+}
+
 // distance_filter (src/Tagore_src.cu:1488-1490) as nvcc compiles it, one fused
 // multiply-add, and angle_filter (:1493-1495) with IEEE-rounded operations.
 __device__ __forceinline__ bool pruned_by(int metric, float res, float dis, float cur, float thre) {

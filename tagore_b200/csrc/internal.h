@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
+#include <vector>
 
 #include "../../include/tagore_b200.h"
 
@@ -106,6 +108,15 @@ struct KnnStats {
 };
 // Builds the kNN graph over d.data (FP16 base) into d.graph / d.nd.
 int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, cudaStream_t s);
+
+// ---- largeIndex (large_index.cpp) ----
+// Builds cluster `cid` (global ids `ids`) into n x K rows [deg, global ids..]
+// and reports its entry point as a global id.
+using LargeBuildFn = std::function<int(const TagoreLargeParams&, uint32_t cid,
+                                       const std::vector<uint32_t>& ids,
+                                       std::vector<uint32_t>& rows, uint32_t* medoid)>;
+int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int ndev,
+                    const LargeBuildFn& build);
 
 // ---- base preparation (prep.cu) ----
 // FP16 base = raw * factor (as __float2half) and exact FP32 squared norms of

@@ -130,6 +130,12 @@ __device__ __forceinline__ void propose(unsigned long long* pool, uint32_t a, ui
 template <int D>
 __device__ __forceinline__ float thread_dist(const uint32_t* __restrict__ a,
                                              const uint32_t* __restrict__ b, uint32_t dim_rt) {
+  if constexpr (D > 0) {
+    return serial_dist<D>([&](int j, int w) {
+      const uint32_t* r = w ? b : a;
+      return make_uint2(r[2 * j], r[2 * j + 1]);
+    });
+  }
   float x[32], y[32];
 #pragma unroll
   for (int l = 0; l < 32; ++l) {

@@ -1,0 +1,390 @@
+// large_index.cpp -- single-device largeIndex (pybind.cu:298-391,
+// src/large_index.cu): every point sits in two clusters; each cluster's local
+// graph is built on the GPU (kNN graph without rescale, CFS path prune with
+// alpha = thre), remapped to global ids and handed to a host merger that keeps
+// `buffer_size` local graphs in memory, merges the two copies of a point when
+// both are resident, spills evicted local graphs to local_prefix + cid, and
+// finally streams the DiskANN-style index.
+//
+// The builder (this thread, the GPU) runs ahead of the merger (a host thread)
+// through a bounded queue; every wait between them is bounded and ends in
+// TAGORE_ETIMEOUT. The merged bytes equal a sequential run of the reference's
+// merger (order_merge_new, :286-522) over the same local graphs.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <functional>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "internal.h"
+
+namespace tagore {
+namespace {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+
+// Greedy cluster order of reorder() (src/large_index.cu:9-83, "Algorithm 4"):
+// fill the buffer with the clusters overlapping most with those already
+// chosen, then repeatedly pick the cluster and the slot whose eviction keeps
+// the largest overlap. Defined here where the reference reads an unset index
+// (no positive overlap anywhere): the smallest unchosen cluster, slot 0.
+void cluster_order(const std::vector<uint32_t>& inter, uint32_t C, uint32_t bs,
+                   std::vector<uint32_t>& order, std::vector<uint32_t>& position) {
+  order.clear();
+  position.assign(C, 0);
+  std::vector<uint8_t> visited(C, 0);
+  std::vector<uint32_t> buffer;
+  order.push_back(0);
+  visited[0] = 1;
+  buffer.push_back(0);
+  position[0] = 0;
+  auto first_free = [&]() {
+    for (uint32_t j = 0; j < C; ++j)
+      if (!visited[j]) return j;
+    return kNone;
+  };
+  for (uint32_t i = 1; i < bs; ++i) {
+    uint64_t max_sum = 0;
+    uint32_t max_id = kNone;
+    for (uint32_t j = 0; j < C; ++j) {
+      if (visited[j]) continue;
+      uint64_t t = 0;
+      for (uint32_t r : order) t += inter[(size_t)j * C + r];
+      if (t > max_sum) {
+        max_sum = t;
+        max_id = j;
+      }
+    }
+    if (max_id == kNone) max_id = first_free();
+    order.push_back(max_id);
+    buffer.push_back(max_id);
+    position[max_id] = i;
+    visited[max_id] = 1;
+  }
+  for (uint32_t i = 0; i + bs < C; ++i) {
+    uint64_t max_sum = 0;
+    uint32_t max_id = kNone, max_evict = 0;
+    for (uint32_t j = 0; j < C; ++j) {
+      if (visited[j]) continue;
+      uint64_t total = 0;
+      for (uint32_t k = 0; k < bs; ++k) total += inter[(size_t)j * C + buffer[k]];
+      uint64_t best = 0;
+      uint32_t best_k = kNone;
+      for (uint32_t k = 0; k < bs; ++k) {
+        const uint64_t t = total - inter[(size_t)j * C + buffer[k]];  // all slots but k
+        if (t > best) {
+          best = t;
+          best_k = k;
+        }
+      }
+      if (best > max_sum) {
+        max_sum = best;
+        max_id = j;
+        max_evict = best_k;
+      }
+    }
+    if (max_id == kNone) {
+      max_id = first_free();
+      max_evict = 0;
+    }
+    buffer[max_evict] = max_id;
+    order.push_back(max_id);
+    visited[max_id] = 1;
+    position[max_id] = max_evict;
+  }
+}
+
+struct Built {
+  std::vector<uint32_t> rows;  // n x K, [deg, global ids...]
+  uint32_t medoid = 0;
+  bool ready = false;
+};
+
+struct Shared {
+  std::mutex mu;
+  std::condition_variable cv;
+  std::vector<Built> built;  // by processing index
+  uint32_t consumed = 0;     // clusters the merger has taken
+  int error = TAGORE_OK;
+  std::string msg;
+};
+
+bool wait_for(Shared& sh, std::unique_lock<std::mutex>& lk, const std::function<bool()>& pred) {
+  return sh.cv.wait_for(lk, std::chrono::seconds(1800), [&] { return pred() || sh.error; });
+}
+
+struct Writer {
+  FILE* f = nullptr;
+  std::vector<char> buf;
+  explicit Writer(const std::string& p) {
+    f = std::fopen(p.c_str(), "wb");
+    if (f) {
+      buf.resize(8u << 20);
+      std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+    }
+  }
+  bool put(const void* p, size_t n) { return n == 0 || std::fwrite(p, 1, n, f) == n; }
+  bool close() {
+    const bool ok = f && std::fclose(f) == 0;
+    f = nullptr;
+    return ok;
+  }
+  ~Writer() {
+    if (f) std::fclose(f);
+  }
+};
+
+struct Reader {
+  FILE* f = nullptr;
+  std::vector<char> buf;
+  bool open(const std::string& p) {
+    f = std::fopen(p.c_str(), "rb");
+    if (f) {
+      buf.resize(1u << 20);
+      std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+    }
+    return f != nullptr;
+  }
+  bool get(void* p, size_t n) { return n == 0 || std::fread(p, 1, n, f) == n; }
+  ~Reader() {
+    if (f) std::fclose(f);
+  }
+};
+
+// The merger of order_merge_new (src/large_index.cu:286-522), sequentially.
+int merge_all(const TagoreLargeParams& p, const std::vector<std::vector<uint32_t>>& clusters,
+              const std::vector<uint32_t>& centers, const std::vector<uint32_t>& second,
+              const std::vector<uint32_t>& order, const std::vector<uint32_t>& position,
+              Shared& sh) {
+  const uint32_t C = (uint32_t)clusters.size(), N = p.num, K = p.k, bs = p.buffer_size;
+  const uint32_t maxd = p.max_degree;
+  std::vector<std::vector<uint32_t>> pool(bs);
+  std::vector<uint32_t> buffer(bs, kNone), pointers(N, 0), medoids(C, 0);
+  std::vector<uint8_t> visited(N, 0), node_set(N, 0), cached(N, 0);
+  std::vector<uint32_t> nhood;
+  auto take = [&](uint32_t i) -> int {
+    std::unique_lock<std::mutex> lk(sh.mu);
+    if (!wait_for(sh, lk, [&] { return sh.built[i].ready; }))
+      return fail(TAGORE_ETIMEOUT, "largeIndex: cluster %u was not built in time", order[i]);
+    if (sh.error) return sh.error;
+    pool[position[order[i]]].swap(sh.built[i].rows);
+    medoids[i] = sh.built[i].medoid;
+    sh.consumed = i + 1;
+    sh.cv.notify_all();
+    return TAGORE_OK;
+  };
+  auto row = [&](uint32_t cid, uint32_t j) { return pool[position[cid]].data() + (size_t)j * K; };
+  auto spill = [&](uint32_t cid) -> int {
+    Writer w(std::string(p.local_prefix) + std::to_string(cid));
+    if (!w.f) return fail(TAGORE_EIO, "cannot create local index for cluster %u", cid);
+    for (uint32_t j = 0; j < clusters[cid].size(); ++j) {
+      const uint32_t* r = row(cid, j);
+      if (!w.put(r, 4) || !w.put(r + 1, 4ull * r[0]))
+        return fail(TAGORE_EIO, "write of local index %u failed", cid);
+      visited[clusters[cid][j]] = 1;
+      pointers[clusters[cid][j]] = kNone;
+    }
+    if (!w.close()) return fail(TAGORE_EIO, "write of local index %u failed", cid);
+    return TAGORE_OK;
+  };
+  TG_TRY(take(0));
+  for (uint32_t j = 0; j < clusters[order[0]].size(); ++j) {
+    visited[clusters[order[0]][j]] = 1;
+    pointers[clusters[order[0]][j]] = j;
+  }
+  buffer[0] = order[0];
+  for (uint32_t i = 1; i < C; ++i) {
+    TG_TRY(take(i));
+    const uint32_t cur = order[i];
+    for (uint32_t j = 0; j < clusters[cur].size(); ++j) {
+      const uint32_t node = clusters[cur][j];
+      if (!visited[node]) {
+        visited[node] = 1;
+        pointers[node] = j;
+        continue;
+      }
+      if (pointers[node] == kNone) continue;  // the other copy went to disk
+      const uint32_t ano = centers[node] == cur ? second[node] : centers[node];
+      uint32_t* old_r = row(ano, pointers[node]);
+      uint32_t* new_r = row(cur, j);
+      // the copy in the point's first cluster goes first (:332-368)
+      const uint32_t* first = centers[node] != cur ? old_r : new_r;
+      const uint32_t* then = centers[node] != cur ? new_r : old_r;
+      nhood.clear();
+      for (uint32_t k = 1; k <= first[0]; ++k) {
+        node_set[first[k]] = 1;
+        nhood.push_back(first[k]);
+      }
+      for (uint32_t k = 1; k <= then[0]; ++k)
+        if (!node_set[then[k]]) {
+          node_set[then[k]] = 1;
+          nhood.push_back(then[k]);
+        }
+      const uint32_t deg = std::min<uint32_t>((uint32_t)nhood.size(), maxd);
+      for (uint32_t k = 1; k <= deg; ++k) old_r[k] = nhood[k - 1];
+      old_r[0] = deg;
+      new_r[0] = 0;
+      for (uint32_t v : nhood) node_set[v] = 0;
+      cached[node] = 1;
+    }
+    buffer[position[cur]] = cur;
+    if (i + 1 >= bs && i + 1 < C) {
+      const uint32_t evict = buffer[position[order[i + 1]]];
+      if (evict != kNone) TG_TRY(spill(evict));
+    }
+  }
+  for (uint32_t s = 0; s < bs; ++s)
+    if (buffer[s] != kNone) TG_TRY(spill(buffer[s]));
+  pool.clear();
+
+  // Final merge into the index file (:447-520).
+  Writer out(p.index_store_path);
+  if (!out.f) return fail(TAGORE_EIO, "cannot create '%s'", p.index_store_path);
+  uint64_t index_size = 0;
+  bool ok = out.put(&index_size, 8) && out.put(&maxd, 4) && out.put(&maxd, 4) && out.put(&index_size, 8);
+  std::vector<Reader> shard(C);
+  for (uint32_t c = 0; c < C; ++c)
+    if (!shard[c].open(std::string(p.local_prefix) + std::to_string(c)))
+      return fail(TAGORE_EIO, "cannot open local index of cluster %u", c);
+  std::vector<uint32_t> a(K), b(K);
+  for (uint32_t i = 0; ok && i < N; ++i) {
+    uint32_t d1 = 0, d2 = 0;
+    if (cached[i]) {
+      uint32_t cid = centers[i];
+      ok = shard[cid].get(&d1, 4);
+      if (ok && d1 == 0) {
+        cid = second[i];
+        ok = shard[cid].get(&d1, 4);
+      } else if (ok) {
+        ok = shard[second[i]].get(&d2, 4);
+      }
+      if (d1 > K) return fail(TAGORE_EIO, "corrupt local index record");
+      ok = ok && shard[cid].get(a.data(), 4ull * d1) && out.put(&d1, 4) && out.put(a.data(), 4ull * d1);
+      index_size += 4ull * (1 + d1);
+    } else {
+      ok = shard[centers[i]].get(&d1, 4) && d1 <= K && shard[centers[i]].get(a.data(), 4ull * d1) &&
+           shard[second[i]].get(&d2, 4) && d2 <= K && shard[second[i]].get(b.data(), 4ull * d2);
+      if (!ok) break;
+      nhood.clear();
+      for (uint32_t j = 0; j < d1; ++j) {
+        node_set[a[j]] = 1;
+        nhood.push_back(a[j]);
+      }
+      for (uint32_t j = 0; j < d2; ++j)
+        if (!node_set[b[j]]) {
+          node_set[b[j]] = 1;
+          nhood.push_back(b[j]);
+        }
+      for (uint32_t v : nhood) node_set[v] = 0;
+      const uint32_t deg = std::min<uint32_t>((uint32_t)nhood.size(), maxd);
+      ok = out.put(&deg, 4) && out.put(nhood.data(), 4ull * deg);
+      index_size += 4ull * (1 + deg);
+    }
+  }
+  if (!ok) return fail(TAGORE_EIO, "reading local indexes or writing '%s' failed", p.index_store_path);
+  index_size += 24;
+  // header: size, max degree, medoid of the last cluster built (:516-519)
+  if (std::fflush(out.f) != 0 || std::fseek(out.f, 0, SEEK_SET) != 0 || !out.put(&index_size, 8) ||
+      !out.put(&maxd, 4) || !out.put(&medoids[C - 1], 4) || !out.close())
+    return fail(TAGORE_EIO, "write to '%s' failed", p.index_store_path);
+  return TAGORE_OK;
+}
+
+}  // namespace
+
+int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int ndev,
+                    const LargeBuildFn& build) {
+  if (!p.data_prefix || !p.local_prefix || !p.index_store_path || !p.centers_path)
+    return fail(TAGORE_EINVAL, "largeIndex: null path");
+  if (ndev != 1)
+    return fail(TAGORE_EINVAL, "largeIndex runs on one device here (devicelist must hold one id)");
+  (void)dev_list;
+  const uint32_t C = p.cluster_num, N = p.num;
+  if (C == 0 || N == 0 || p.buffer_size == 0 || p.k == 0 || p.max_degree == 0 || p.max_degree >= p.k)
+    return fail(TAGORE_EINVAL, "largeIndex: need clusters, points, buffer_size > 0 and max_degree < K");
+  FILE* f = std::fopen(p.centers_path, "rb");
+  if (!f) return fail(TAGORE_EIO, "cannot open '%s'", p.centers_path);
+  std::vector<uint32_t> cc((size_t)N * 2);
+  const size_t got = std::fread(cc.data(), 4, cc.size(), f);
+  std::fclose(f);
+  if (got != cc.size()) return fail(TAGORE_EIO, "'%s' holds fewer than %u center pairs", p.centers_path, N);
+  std::vector<uint32_t> centers(N), second(N);
+  std::vector<std::vector<uint32_t>> clusters(C);
+  for (uint32_t i = 0; i < N; ++i) {
+    centers[i] = cc[2 * i];
+    second[i] = cc[2 * i + 1];
+    if (centers[i] >= C || second[i] >= C) return fail(TAGORE_EINVAL, "point %u names a cluster >= %u", i, C);
+  }
+  for (uint32_t i = 0; i < N; ++i) {
+    clusters[centers[i]].push_back(i);
+    clusters[second[i]].push_back(i);
+  }
+  for (uint32_t c = 0; c < C; ++c) {
+    if (clusters[c].size() > p.max_points)
+      return fail(TAGORE_EINVAL,
+                  "cluster %u holds %zu points > max_points %u (the reference splits it into "
+                  "clusters that have no data file)",
+                  c, clusters[c].size(), p.max_points);
+    if (clusters[c].size() <= p.k)
+      return fail(TAGORE_EINVAL, "cluster %u holds %zu points, not more than K = %u", c,
+                  clusters[c].size(), p.k);
+  }
+  std::vector<uint32_t> inter((size_t)C * C, 0);  // order_merge_main (:86-106)
+  for (uint32_t i = 0; i < N; ++i) {
+    ++inter[(size_t)centers[i] * C + second[i]];
+    ++inter[(size_t)second[i] * C + centers[i]];
+  }
+  TagoreLargeParams q = p;
+  q.buffer_size = std::min(p.buffer_size, C);
+  std::vector<uint32_t> order, position;
+  cluster_order(inter, C, q.buffer_size, order, position);
+
+  Shared sh;
+  sh.built.resize(C);
+  int merge_rc = TAGORE_OK;
+  std::string merge_msg;
+  std::thread merger([&]() {
+    merge_rc = merge_all(q, clusters, centers, second, order, position, sh);
+    if (merge_rc != TAGORE_OK) merge_msg = tagore_last_error();
+    std::lock_guard<std::mutex> g(sh.mu);
+    if (merge_rc != TAGORE_OK && !sh.error) sh.error = merge_rc;
+    sh.cv.notify_all();
+  });
+  const uint32_t ahead = 2;  // clusters built but not yet merged
+  int rc = TAGORE_OK;
+  for (uint32_t i = 0; i < C && rc == TAGORE_OK; ++i) {
+    {
+      std::unique_lock<std::mutex> lk(sh.mu);
+      if (!wait_for(sh, lk, [&] { return sh.consumed + ahead > i; })) {
+        rc = fail(TAGORE_ETIMEOUT, "largeIndex: merger stalled");
+        break;
+      }
+      if (sh.error) break;
+    }
+    const uint32_t cid = order[i];
+    std::vector<uint32_t> rows;
+    uint32_t medoid = 0;
+    rc = build(q, cid, clusters[cid], rows, &medoid);
+    std::lock_guard<std::mutex> g(sh.mu);
+    if (rc != TAGORE_OK) {
+      sh.error = rc;
+      sh.msg = tagore_last_error();
+    } else {
+      sh.built[i].rows.swap(rows);
+      sh.built[i].medoid = medoid;
+      sh.built[i].ready = true;
+    }
+    sh.cv.notify_all();
+  }
+  merger.join();
+  if (rc != TAGORE_OK) return fail(rc, "%s", sh.msg.empty() ? tagore_last_error() : sh.msg.c_str());
+  if (merge_rc != TAGORE_OK) return fail(merge_rc, "%s", merge_msg.c_str());
+  return TAGORE_OK;
+}
+
+}  // namespace tagore

@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "internal.h"
+#include "knn_shared.cuh"
 
 namespace tagore {
 namespace {
@@ -36,10 +37,119 @@ __device__ __forceinline__ uint32_t align4(uint32_t x) { return (x + 3u) & ~3u; 
 struct Beam {
   uint32_t* id;
   float* dis;
-  uint32_t* id2;
   uint8_t* ex;
+  uint32_t* hash;  // membership set of the W beam ids (open addressing)
 };
+constexpr uint32_t kHash = 512;  // >= 4/3 of the largest beam (TOPM <= 256, K <= 128)
 
+__host__ __device__ inline size_t beam_bytes(uint32_t W) {
+  return (size_t)W * 8 + ((W + 15u) & ~15u) + (size_t)kHash * 4;
+}
+
+__device__ inline Beam beam_carve(unsigned char* p, uint32_t W) {
+  Beam b;
+  b.hash = reinterpret_cast<uint32_t*>(p);
+  b.id = b.hash + kHash;
+  b.dis = reinterpret_cast<float*>(b.id + W);
+  b.ex = reinterpret_cast<uint8_t*>(b.dis + W);
+  return b;
+}
+
+__device__ __forceinline__ uint32_t hslot(uint32_t key) { return (key * 0x9E3779B1u) >> 23; }
+
+// The reference keeps the beam ids sorted (top_M_Cand2, :1253-1259) only to
+// test membership (:1282-1290); a hash set of the same ids answers the same
+// question without a 36-pass sort per expansion.
+__device__ void beam_rehash(Beam bm, uint32_t W, int lane) {
+  for (uint32_t t = lane; t < kHash; t += 32) bm.hash[t] = kInv;
+  __syncwarp();
+  for (uint32_t t = lane; t < W; t += 32) {
+    const uint32_t key = bm.id[t];
+    if (key == kInv) continue;
+    uint32_t h = hslot(key);
+    while (true) {
+      const uint32_t prev = atomicCAS(&bm.hash[h], kInv, key);
+      if (prev == kInv || prev == key) break;
+      h = (h + 1) & (kHash - 1);
+    }
+  }
+  __syncwarp();
+}
+
+__device__ __forceinline__ bool beam_has(const Beam& bm, uint32_t key) {
+  uint32_t h = hslot(key);
+  while (true) {
+    const uint32_t v = bm.hash[h];
+    if (v == key) return true;
+    if (v == kInv) return false;
+    h = (h + 1) & (kHash - 1);
+  }
+}
+
+// Sorts (dis, id, ex) over [off, off+len) exactly as the reference network
+// does wherever the result is observable: positions [off, off+keep) plus the
+// set of ids. With strictly increasing distances over those positions every
+// correct sort agrees with the network, so a register bitonic sort on
+// (distance, position) is used and checked; on a tie the network runs on the
+// untouched input.
+__device__ void beam_sort(Beam bm, uint32_t off, uint32_t len, uint32_t keep, int lane) {
+  if (len <= 256) {
+    uint64_t key[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const uint32_t p = lane + 32 * t;
+      key[t] = p < len ? (((uint64_t)__float_as_uint(bm.dis[off + p]) << 32) | p) : ~0ull;
+    }
+    knn::warp_sort_keys<8>(key, lane);
+    // strict increase over the first min(keep+1, len) sorted positions
+    bool tie = false;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const uint32_t p = lane + 32 * t;
+      uint64_t prev = __shfl_up_sync(kFull, (uint32_t)(key[t] >> 32), 1);
+      if (t > 0) {
+        const uint32_t tail = __shfl_sync(kFull, (uint32_t)(key[t - 1] >> 32), 31);
+        if (lane == 0) prev = tail;
+      }
+      if (p >= 1 && p <= keep && p < len && (uint32_t)(key[t] >> 32) == (uint32_t)prev) tie = true;
+    }
+    if (!__any_sync(kFull, tie)) {
+      uint32_t vid[8], vex[8];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const uint32_t p = lane + 32 * t;
+        if (p < len) {
+          const uint32_t src = off + (uint32_t)(key[t] & 0xFFFFFFFFu);
+          vid[t] = bm.id[src];
+          vex[t] = bm.ex[src];
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const uint32_t p = lane + 32 * t;
+        if (p < len) {
+          bm.dis[off + p] = __uint_as_float((uint32_t)(key[t] >> 32));
+          bm.id[off + p] = vid[t];
+          bm.ex[off + p] = (uint8_t)vex[t];
+        }
+      }
+      __syncwarp();
+      return;
+    }
+  }
+  float* D = bm.dis + off;
+  uint32_t* I = bm.id + off;
+  uint8_t* E = bm.ex + off;
+  warp_network(len, lane, [&](uint32_t u, uint32_t d) { return D[u] > D[d]; },
+               [&](uint32_t u, uint32_t d) {
+                 swap_(D[u], D[d]);
+                 swap_(I[u], I[d]);
+                 swap_(E[u], E[d]);
+               });
+}
+
+// Beam search shared by cal_ep_gpu (:1905-2047) and collect_path (:1211-1335).
 __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __restrict__ data,
                               uint32_t dim, uint32_t K, const __half* query, uint32_t start,
                               uint32_t topm, uint32_t iters, Beam bm, uint32_t* ring_id,
@@ -75,17 +185,8 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     }
   }
   __syncwarp();
-  {
-    float* D = bm.dis + topm;
-    uint32_t* I = bm.id + topm;
-    uint8_t* E = bm.ex + topm;
-    warp_network(K, lane, [&](uint32_t u, uint32_t d) { return D[u] > D[d]; },
-                 [&](uint32_t u, uint32_t d) {
-                   swap_(D[u], D[d]);
-                   swap_(I[u], I[d]);
-                   swap_(E[u], E[d]);
-                 });
-  }
+  // The seed sort is observable on its first min(TOPM, K) positions.
+  beam_sort(bm, topm, K, min(topm, K), lane);
   for (uint32_t i = lane; i < topm; i += 32) {
     if (topm + i < W) {
       bm.id[i] = bm.id[topm + i];
@@ -98,13 +199,7 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     }
   }
   __syncwarp();
-  auto rebuild_id2 = [&]() {
-    for (uint32_t t = lane; t < W; t += 32) bm.id2[t] = bm.id[t];
-    __syncwarp();
-    warp_network(W, lane, [&](uint32_t u, uint32_t d) { return bm.id2[u] > bm.id2[d]; },
-                 [&](uint32_t u, uint32_t d) { swap_(bm.id2[u], bm.id2[d]); });
-  };
-  rebuild_id2();
+  beam_rehash(bm, W, lane);
   uint32_t curr = K, to_explore = kInv;
   for (uint32_t it = 0; it < iters; ++it) {
     // First unexplored of the top TOPM; when none is left the reference keeps
@@ -124,7 +219,7 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     if (to_explore == kInv) break;
     for (uint32_t j = lane; j < K; j += 32) {
       const uint32_t a = __ldg(G + (size_t)to_explore * K + j);
-      bm.dis[topm + j] = sorted_contains(bm.id2, W, a) ? kInfDis : 0.0f;
+      bm.dis[topm + j] = beam_has(bm, a) ? kInfDis : 0.0f;
       bm.id[topm + j] = a;
       bm.ex[topm + j] = 0;
     }
@@ -162,13 +257,10 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     }
     if (np) flush();
     __syncwarp();
-    warp_network(W, lane, [&](uint32_t u, uint32_t d) { return bm.dis[u] > bm.dis[d]; },
-                 [&](uint32_t u, uint32_t d) {
-                   swap_(bm.dis[u], bm.dis[d]);
-                   swap_(bm.id[u], bm.id[d]);
-                   swap_(bm.ex[u], bm.ex[d]);
-                 });
-    rebuild_id2();
+    // Positions >= TOPM are overwritten by the next expansion; only [0, TOPM)
+    // and the id set survive.
+    beam_sort(bm, 0, W, topm, lane);
+    beam_rehash(bm, W, lane);
   }
   if (ring_count) *ring_count = curr;
   return bm.id[0];
@@ -264,7 +356,7 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
 struct SelLayout {
   uint32_t W, L, fd;
   __host__ __device__ size_t bytes() const {
-    return (size_t)W * 12 + ((W + 15u) & ~15u) + (size_t)L * 8 + (size_t)fd * 8 + 64;
+    return (W ? beam_bytes(W) : 0) + (size_t)L * 8 + (size_t)fd * 8 + 64;
   }
 };
 
@@ -282,11 +374,7 @@ __global__ void k_cal_ep(const uint32_t* __restrict__ G, const __half* __restric
                          uint32_t topm, uint32_t* ep) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t W = topm + K;
-  Beam bm;
-  bm.id = reinterpret_cast<uint32_t*>(smem);
-  bm.dis = reinterpret_cast<float*>(bm.id + W);
-  bm.id2 = reinterpret_cast<uint32_t*>(bm.dis + W);
-  bm.ex = reinterpret_cast<uint8_t*>(bm.id2 + W);
+  Beam bm = beam_carve(smem, W);
   const int lane = threadIdx.x & 31;
   if (threadIdx.x >= 32) return;
   const uint32_t best = warp_beam(G, data, dim, K, center, 0, topm, 30, bm, nullptr, nullptr,
@@ -311,11 +399,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   float* cdis = reinterpret_cast<float*>(cand + lay.L);
   uint32_t* sel = reinterpret_cast<uint32_t*>(cdis + lay.L);
   float* seld = reinterpret_cast<float*>(sel + fd);
-  Beam bm;
-  bm.id = reinterpret_cast<uint32_t*>(seld + fd);
-  bm.dis = reinterpret_cast<float*>(bm.id + lay.W);
-  bm.id2 = reinterpret_cast<uint32_t*>(bm.dis + lay.W);
-  bm.ex = reinterpret_cast<uint8_t*>(bm.id2 + lay.W);
+  Beam bm = beam_carve(reinterpret_cast<unsigned char*>(seld + fd), lay.W);
   const uint32_t L = lay.L;
   const uint32_t ep = kPath ? *ep_dev : 0u;
   for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
@@ -791,9 +875,12 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   uint32_t* ep_dev = P_cnt + d.n;
   if (path) {
     const uint32_t W = a.topm + K;
-    const size_t sm = (size_t)W * 12 + ((W + 15u) & ~15u) + 64;
+    const size_t sm = beam_bytes(W) + 64;
     TG_TRY(set_smem((const void*)k_cal_ep, sm));
+    stage_begin("prune_cal_ep", s);
     k_cal_ep<<<1, 32, sm, s>>>(d.graph, d.data, d.center, d.dim, K, a.topm, ep_dev);
+    count_launch();
+    stage_end("prune_cal_ep", s);
     TG_CUDA(cudaGetLastError());
   }
   SelLayout lay{path ? a.topm + K : 0u, kSelectCand + K, fd};
@@ -801,18 +888,27 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   const void* fn = path ? (const void*)k_select<true> : (const void*)k_select<false>;
   TG_TRY(set_smem(fn, sm));
   const int grid = grid_for(kWarps, d.n);
+  const char* sel_name = path ? "prune_select_path" : "prune_select_2hop";
+  stage_begin(sel_name, s);
   if (path)
     k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
                                                  a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
   else
     k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
                                                   a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+  count_launch();
+  stage_end(sel_name, s);
   TG_CUDA(cudaGetLastError());
+  stage_begin("prune_reverse_store", s);
   TG_TRY(reverse_store(d, P_ids, reinterpret_cast<const uint32_t*>(P_dis), P_cnt, fd, 0, K, K, s));
+  stage_end("prune_reverse_store", s);
   const size_t sm2 = ((size_t)(fd + K) * 8 + (size_t)fd * 8 + 16) * kWarps;
   TG_TRY(set_smem((const void*)k_filter_reverse, sm2));
+  stage_begin("prune_filter_reverse", s);
   k_filter_reverse<<<grid, kWarps * 32, sm2, s>>>(d.graph, d.nd, d.rgraph, d.rd, d.rnum, d.data,
                                                   d.n, d.dim, K, fd, metric, a.thre, P_ids, P_cnt);
+  count_launch();
+  stage_end("prune_filter_reverse", s);
   TG_CUDA(cudaGetLastError());
   if (path && ep_host) {
     TG_CUDA(cudaMemcpyAsync(ep_host, ep_dev, 4, cudaMemcpyDeviceToHost, s));
@@ -865,7 +961,7 @@ int stage_cal_ep(const Dev& d, uint32_t topm, uint32_t* ep_host, cudaStream_t s)
   Scratch sc(s);
   TG_TRY(sc.alloc(4));
   const uint32_t W = topm + d.k;
-  const size_t sm = (size_t)W * 12 + ((W + 15u) & ~15u) + 64;
+  const size_t sm = beam_bytes(W) + 64;
   TG_TRY(set_smem((const void*)k_cal_ep, sm));
   k_cal_ep<<<1, 32, sm, s>>>(d.graph, d.data, d.center, d.dim, d.k, topm, sc.as<uint32_t>());
   TG_CUDA(cudaGetLastError());
