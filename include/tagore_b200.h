@@ -106,6 +106,15 @@ int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const cha
  * (pybind.cu:298-391) for a single device (devicelist = [0]). */
 int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev);
 
+/* The host half of largeIndex alone (reorder + order_merge_new,
+ * src/large_index.cu:9-106 and :286-522): the clusters come from
+ * p->centers_path as in tagore_large_index, but each cluster's local graph is
+ * given: local_rows[cid] holds clusters[cid].size() x p->k rows of
+ * [degree, global ids...] and local_medoids[cid] its entry point (a global
+ * id). Writes the spill files and p->index_store_path; no device is used. */
+int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_rows,
+                       const uint32_t* local_medoids);
+
 /* cal_ep_gpu (src/Tagore_src.cu:1889-2058) alone: entry point of the graph
  * held in st (kNN rows) toward st->center. */
 int tagore_entry_point(TagoreKnnState* st, uint32_t topm, uint32_t* ep);

@@ -71,6 +71,7 @@ SIGNATURES = {
     "tagore_pruning_cfs": (C.c_int, [C.POINTER(PruneParams), C.POINTER(KnnState), C.c_char_p,
                                      C.c_char_p]),
     "tagore_large_index": (C.c_int, [C.POINTER(LargeParams), C.c_void_p, C.c_int]),
+    "tagore_large_merge": (C.c_int, [C.POINTER(LargeParams), C.POINTER(C.c_void_p), C.c_void_p]),
     "tagore_entry_point": (C.c_int, [C.POINTER(KnnState), C.c_uint32, C.POINTER(C.c_uint32)]),
     "tagore_state_alloc": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KnnState)]),
     "tagore_state_free": (C.c_int, [C.POINTER(KnnState)]),

@@ -33,111 +33,72 @@ constexpr int kWarps = 4;  // warps (= nodes in flight) per block
 __device__ __forceinline__ uint32_t align4(uint32_t x) { return (x + 3u) & ~3u; }
 
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
 // Beam search shared by cal_ep_gpu (:1905-2047) and collect_path (:1211-1335).
 struct Beam {
   uint32_t* id;
   float* dis;
   uint8_t* ex;
   uint32_t* hash;  // membership set of the W beam ids (open addressing)
+  uint32_t hmask;  // hash slots - 1
+  float* sb;       // scratch: sorted new distances (K)
+  float* sm;       // scratch: merged distances of positions 0..TOPM
 };
-constexpr uint32_t kHash = 512;  // >= 4/3 of the largest beam (TOPM <= 256, K <= 128)
+
+// Hash slots: a power of two holding the beam at load <= 3/4 (TOPM <= 256, K <= 128).
+__host__ __device__ inline uint32_t hash_slots(uint32_t W) { return W <= 192 ? 256u : 512u; }
 
 __host__ __device__ inline size_t beam_bytes(uint32_t W) {
-  return (size_t)W * 8 + ((W + 15u) & ~15u) + (size_t)kHash * 4;
+  return (size_t)hash_slots(W) * 4 + (size_t)W * 8 + ((W + 15u) & ~15u) + 128 * 4 +
+         (size_t)(W + 1) * 4;
 }
 
 __device__ inline Beam beam_carve(unsigned char* p, uint32_t W) {
   Beam b;
   b.hash = reinterpret_cast<uint32_t*>(p);
-  b.id = b.hash + kHash;
+  b.hmask = hash_slots(W) - 1;
+  b.id = b.hash + hash_slots(W);
   b.dis = reinterpret_cast<float*>(b.id + W);
-  b.ex = reinterpret_cast<uint8_t*>(b.dis + W);
+  b.sb = b.dis + W;
+  b.sm = b.sb + 128;
+  b.ex = reinterpret_cast<uint8_t*>(b.sm + W + 1);
   return b;
 }
 
-__device__ __forceinline__ uint32_t hslot(uint32_t key) { return (key * 0x9E3779B1u) >> 23; }
+__device__ __forceinline__ uint32_t hslot(uint32_t key, uint32_t mask) {
+  return ((key * 0x9E3779B1u) >> 23) & mask;
+}
 
 // The reference keeps the beam ids sorted (top_M_Cand2, :1253-1259) only to
 // test membership (:1282-1290); a hash set of the same ids answers the same
-// question without a 36-pass sort per expansion.
+// question without a sort.
 __device__ void beam_rehash(Beam bm, uint32_t W, int lane) {
-  for (uint32_t t = lane; t < kHash; t += 32) bm.hash[t] = kInv;
+  for (uint32_t t = lane; t <= bm.hmask; t += 32) bm.hash[t] = kInv;
   __syncwarp();
   for (uint32_t t = lane; t < W; t += 32) {
     const uint32_t key = bm.id[t];
     if (key == kInv) continue;
-    uint32_t h = hslot(key);
+    uint32_t h = hslot(key, bm.hmask);
     while (true) {
       const uint32_t prev = atomicCAS(&bm.hash[h], kInv, key);
       if (prev == kInv || prev == key) break;
-      h = (h + 1) & (kHash - 1);
+      h = (h + 1) & bm.hmask;
     }
   }
   __syncwarp();
 }
 
 __device__ __forceinline__ bool beam_has(const Beam& bm, uint32_t key) {
-  uint32_t h = hslot(key);
+  uint32_t h = hslot(key, bm.hmask);
   while (true) {
     const uint32_t v = bm.hash[h];
     if (v == key) return true;
     if (v == kInv) return false;
-    h = (h + 1) & (kHash - 1);
+    h = (h + 1) & bm.hmask;
   }
 }
 
-// Sorts (dis, id, ex) over [off, off+len) exactly as the reference network
-// does wherever the result is observable: positions [off, off+keep) plus the
-// set of ids. With strictly increasing distances over those positions every
-// correct sort agrees with the network, so a register bitonic sort on
-// (distance, position) is used and checked; on a tie the network runs on the
-// untouched input.
-__device__ void beam_sort(Beam bm, uint32_t off, uint32_t len, uint32_t keep, int lane) {
-  if (len <= 256) {
-    uint64_t key[8];
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const uint32_t p = lane + 32 * t;
-      key[t] = p < len ? (((uint64_t)__float_as_uint(bm.dis[off + p]) << 32) | p) : ~0ull;
-    }
-    knn::warp_sort_keys<8>(key, lane);
-    // strict increase over the first min(keep+1, len) sorted positions
-    bool tie = false;
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const uint32_t p = lane + 32 * t;
-      uint64_t prev = __shfl_up_sync(kFull, (uint32_t)(key[t] >> 32), 1);
-      if (t > 0) {
-        const uint32_t tail = __shfl_sync(kFull, (uint32_t)(key[t - 1] >> 32), 31);
-        if (lane == 0) prev = tail;
-      }
-      if (p >= 1 && p <= keep && p < len && (uint32_t)(key[t] >> 32) == (uint32_t)prev) tie = true;
-    }
-    if (!__any_sync(kFull, tie)) {
-      uint32_t vid[8], vex[8];
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const uint32_t p = lane + 32 * t;
-        if (p < len) {
-          const uint32_t src = off + (uint32_t)(key[t] & 0xFFFFFFFFu);
-          vid[t] = bm.id[src];
-          vex[t] = bm.ex[src];
-        }
-      }
-      __syncwarp();
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const uint32_t p = lane + 32 * t;
-        if (p < len) {
-          bm.dis[off + p] = __uint_as_float((uint32_t)(key[t] >> 32));
-          bm.id[off + p] = vid[t];
-          bm.ex[off + p] = (uint8_t)vex[t];
-        }
-      }
-      __syncwarp();
-      return;
-    }
-  }
+__device__ void beam_network(Beam bm, uint32_t off, uint32_t len, int lane) {
   float* D = bm.dis + off;
   uint32_t* I = bm.id + off;
   uint8_t* E = bm.ex + off;
@@ -149,7 +110,133 @@ __device__ void beam_sort(Beam bm, uint32_t off, uint32_t len, uint32_t keep, in
                });
 }
 
-// Beam search shared by cal_ep_gpu (:1905-2047) and collect_path (:1211-1335).
+// Sorted (distance, position) keys of the n <= 128 entries at [off, off+n),
+// element-major in four registers per lane.
+__device__ __forceinline__ void sorted_keys(const Beam& bm, uint32_t off, uint32_t n, uint64_t (&key)[4],
+                                            int lane) {
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const uint32_t j = lane + 32 * t;
+    key[t] = j < n ? (((uint64_t)__float_as_uint(bm.dis[off + j]) << 32) | j) : ~0ull;
+  }
+  knn::warp_sort_keys<4>(key, lane);
+}
+
+__device__ __forceinline__ float key_dis(uint64_t k) { return __uint_as_float((uint32_t)(k >> 32)); }
+
+// After an expansion: [0, topm) holds the previous sorted prefix, [topm, W)
+// the K new entries. The reference sorts all W with its network; only
+// [0, topm) and the set of the W ids survive into the next expansion (the
+// rest is overwritten), and with strictly increasing distances over merged
+// positions 0..topm that part is the same for every correct sort. So the new
+// entries are sorted in registers and merged into the prefix by rank; a tie
+// there falls back to the network.
+__device__ void beam_update(Beam bm, uint32_t topm, uint32_t K, int lane) {
+  const uint32_t W = topm + K;
+  if (topm > 128 || K > 128) {
+    beam_network(bm, 0, W, lane);
+    beam_rehash(bm, W, lane);
+    return;
+  }
+  beam_rehash(bm, W, lane);  // the set of all W ids, before anything moves
+  uint64_t key[4];
+  sorted_keys(bm, topm, K, key, lane);
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const uint32_t p = lane + 32 * t;
+    if (p < K) bm.sb[p] = key_dis(key[t]);
+  }
+  __syncwarp();
+  // ranks: prefix i -> i + #(new < A_i); new p -> p + #(prefix <= B_p)
+  uint32_t ra[4], rb[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const uint32_t i = lane + 32 * t;
+    ra[t] = kInv;
+    if (i < topm) {
+      const float a = bm.dis[i];
+      uint32_t lo = 0, hi = K;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (bm.sb[mid] < a) lo = mid + 1;
+        else hi = mid;
+      }
+      ra[t] = i + lo;
+    }
+    const uint32_t p = lane + 32 * t;
+    rb[t] = kInv;
+    if (p < K) {
+      const float b = key_dis(key[t]);
+      uint32_t lo = 0, hi = topm;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (bm.dis[mid] <= b) lo = mid + 1;
+        else hi = mid;
+      }
+      rb[t] = p + lo;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    if (ra[t] <= topm) bm.sm[ra[t]] = bm.dis[lane + 32 * t];
+    if (rb[t] <= topm) bm.sm[rb[t]] = key_dis(key[t]);
+  }
+  __syncwarp();
+  bool tie = false;
+  for (uint32_t p = lane + 1; p <= topm; p += 32) tie |= bm.sm[p] == bm.sm[p - 1];
+  if (__any_sync(kFull, tie)) {
+    beam_network(bm, 0, W, lane);
+    return;
+  }
+  // gather the survivors' payloads, then write the new prefix
+  uint32_t vid[8], vex[8];
+  float vdis[8];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const uint32_t i = lane + 32 * t;
+    if (ra[t] < topm) {
+      vid[t] = bm.id[i];
+      vex[t] = bm.ex[i];
+      vdis[t] = bm.dis[i];
+    }
+    if (rb[t] < topm) {
+      const uint32_t j = (uint32_t)(key[t] & 0xFFFFFFFFu);
+      vid[4 + t] = bm.id[topm + j];
+      vex[4 + t] = bm.ex[topm + j];
+      vdis[4 + t] = key_dis(key[t]);
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    if (ra[t] < topm) {
+      bm.id[ra[t]] = vid[t];
+      bm.ex[ra[t]] = (uint8_t)vex[t];
+      bm.dis[ra[t]] = vdis[t];
+    }
+    if (rb[t] < topm) {
+      bm.id[rb[t]] = vid[4 + t];
+      bm.ex[rb[t]] = (uint8_t)vex[4 + t];
+      bm.dis[rb[t]] = vdis[4 + t];
+    }
+  }
+  __syncwarp();
+}
+
+// Warms L2 (and L1) with the rows a warp is about to read: lane l covers
+// 128-byte line l of each listed row.
+__device__ __forceinline__ void prefetch_rows(const __half* data, uint32_t dim, const uint32_t* ids,
+                                              uint32_t n, int lane) {
+  const uint32_t lines = (dim * 2 + 127) / 128;
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t id = ids[k];
+    if (id == kInv) continue;
+    const char* row = reinterpret_cast<const char*>(data + (size_t)id * dim);
+    for (uint32_t l = lane; l < lines; l += 32)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128 * l));
+  }
+}
+
 __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __restrict__ data,
                               uint32_t dim, uint32_t K, const __half* query, uint32_t start,
                               uint32_t topm, uint32_t iters, Beam bm, uint32_t* ring_id,
@@ -166,6 +253,7 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     bm.ex[topm + t] = 0;
   }
   __syncwarp();
+  prefetch_rows(data, dim, bm.id + topm, K, lane);
   for (uint32_t i = 0; i < K; i += 4) {
     uint32_t ids[4];
     float d4[4];
@@ -185,17 +273,55 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     }
   }
   __syncwarp();
-  // The seed sort is observable on its first min(TOPM, K) positions.
-  beam_sort(bm, topm, K, min(topm, K), lane);
-  for (uint32_t i = lane; i < topm; i += 32) {
-    if (topm + i < W) {
-      bm.id[i] = bm.id[topm + i];
-      bm.dis[i] = bm.dis[topm + i];
-      bm.ex[i] = bm.ex[topm + i];
-    } else {  // slots past the K seeds start empty (TOPM > K)
-      bm.id[i] = kInv;
-      bm.dis[i] = kInfDis;
-      bm.ex[i] = 1;
+  // Seeds: the network's order is observable on the first min(TOPM, K)
+  // positions, copied into the prefix; a tie there runs the network.
+  const uint32_t keep = min(topm, K);
+  bool seeded = false;
+  if (K <= 128) {
+    uint64_t key[4];
+    sorted_keys(bm, topm, K, key, lane);
+    bool tie = false;
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const uint32_t p = lane + 32 * t;
+      uint32_t prev = __shfl_up_sync(kFull, (uint32_t)(key[t] >> 32), 1);
+      if (t > 0) {
+        const uint32_t tail = __shfl_sync(kFull, (uint32_t)(key[t - 1] >> 32), 31);
+        if (lane == 0) prev = tail;
+      }
+      if (p >= 1 && p <= keep && p < K && (uint32_t)(key[t] >> 32) == prev) tie = true;
+    }
+    if (!__any_sync(kFull, tie)) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const uint32_t p = lane + 32 * t;
+        if (p < keep) {
+          const uint32_t j = (uint32_t)(key[t] & 0xFFFFFFFFu);
+          bm.id[p] = bm.id[topm + j];
+          bm.dis[p] = key_dis(key[t]);
+          bm.ex[p] = 0;
+        }
+      }
+      for (uint32_t i = K + lane; i < topm; i += 32) {  // TOPM > K: empty slots
+        bm.id[i] = kInv;
+        bm.dis[i] = kInfDis;
+        bm.ex[i] = 1;
+      }
+      seeded = true;
+    }
+  }
+  if (!seeded) {
+    beam_network(bm, topm, K, lane);
+    for (uint32_t i = lane; i < topm; i += 32) {
+      if (topm + i < W) {
+        bm.id[i] = bm.id[topm + i];
+        bm.dis[i] = bm.dis[topm + i];
+        bm.ex[i] = bm.ex[topm + i];
+      } else {  // slots past the K seeds start empty (TOPM > K)
+        bm.id[i] = kInv;
+        bm.dis[i] = kInfDis;
+        bm.ex[i] = 1;
+      }
     }
   }
   __syncwarp();
@@ -219,9 +345,15 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     if (to_explore == kInv) break;
     for (uint32_t j = lane; j < K; j += 32) {
       const uint32_t a = __ldg(G + (size_t)to_explore * K + j);
-      bm.dis[topm + j] = beam_has(bm, a) ? kInfDis : 0.0f;
+      const bool member = beam_has(bm, a);
+      bm.dis[topm + j] = member ? kInfDis : 0.0f;
       bm.id[topm + j] = a;
       bm.ex[topm + j] = 0;
+      if (!member) {  // warm L2 with the rows about to be scored
+        const char* row = reinterpret_cast<const char*>(data + (size_t)a * dim);
+        for (uint32_t l = 0; l < (dim * 2 + 127) / 128; ++l)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128 * l));
+      }
     }
     __syncwarp();
     // Distances of the non-members in ascending neighbour order; that order
@@ -257,10 +389,7 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     }
     if (np) flush();
     __syncwarp();
-    // Positions >= TOPM are overwritten by the next expansion; only [0, TOPM)
-    // and the id set survive.
-    beam_sort(bm, 0, W, topm, lane);
-    beam_rehash(bm, W, lane);
+    beam_update(bm, topm, K, lane);
   }
   if (ring_count) *ring_count = curr;
   return bm.id[0];
@@ -311,7 +440,18 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
   }
   __syncwarp();
   uint32_t nsel = 1, last_pos = first;
+  uint32_t warmed = first;  // candidates up to here have their rows warmed
   for (uint32_t i = first + 1; i < len && nsel < fd; ++i) {
+    // keep the next 32 positions' rows on their way into L2
+    if (i + 32 > warmed + 1 && warmed + 1 < len) {
+      const uint32_t p = warmed + 1 + lane;
+      if (p < len && cand[p] != kInv) {
+        const char* row = reinterpret_cast<const char*>(data + (size_t)cand[p] * dim);
+        for (uint32_t l = 0; l < (dim * 2 + 127) / 128; ++l)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128 * l));
+      }
+      warmed = min(len - 1, warmed + 32);
+    }
     const uint32_t c = cand[i];
     if (c == kInv) continue;
     bool dup = false;
@@ -386,7 +526,7 @@ __global__ void k_cal_ep(const uint32_t* __restrict__ G, const __half* __restric
 // path: collect_path + Filter_path(distance_filter); 2-hop: collect_2hop +
 // Filter_path(angle_filter). The reference always uses these two filters.
 template <bool kPath>
-__global__ void __launch_bounds__(kWarps * 32)
+__global__ void __launch_bounds__(kWarps * 32, 8)
     k_select(const uint32_t* __restrict__ G, float* __restrict__ nd, const __half* __restrict__ data,
              uint32_t n, uint32_t dim, uint32_t K, const uint32_t* __restrict__ ep_dev,
              uint32_t topm, uint32_t fd, float thre, uint32_t* __restrict__ P_ids,
@@ -866,7 +1006,7 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
                    cudaStream_t s) {
   const uint32_t fd = a.final_degree, K = d.k;
   if (!path && K * K < kSelectCand) return fail(TAGORE_EINVAL, "2-hop collect needs K*K >= 480");
-  if (path && a.topm == 0) return fail(TAGORE_EINVAL, "TOPM must be >= 1");
+  if (path && (a.topm == 0 || a.topm > 256)) return fail(TAGORE_EINVAL, "TOPM must be in [1, 256]");
   Scratch sc(s);
   TG_TRY(sc.alloc((size_t)d.n * fd * 8 + (size_t)d.n * 4 + 16));
   uint32_t* P_ids = sc.as<uint32_t>();
