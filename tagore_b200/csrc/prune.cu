@@ -525,12 +525,20 @@ __global__ void k_cal_ep(const uint32_t* __restrict__ G, const __half* __restric
 // select_path (:1498-1517) and select_2hop (:1520-1534) into scratch rows.
 // path: collect_path + Filter_path(distance_filter); 2-hop: collect_2hop +
 // Filter_path(angle_filter). The reference always uses these two filters.
+// Node handed to this warp: one shared counter, taken a node at a time, keeps
+// the SMs busy to the end whatever the per-node search length.
+__device__ __forceinline__ uint32_t next_node(uint32_t* ctr, int lane) {
+  uint32_t b = 0;
+  if (lane == 0) b = atomicAdd(ctr, 1u);
+  return __shfl_sync(kFull, b, 0);
+}
+
 template <bool kPath>
 __global__ void __launch_bounds__(kWarps * 32, 8)
     k_select(const uint32_t* __restrict__ G, float* __restrict__ nd, const __half* __restrict__ data,
              uint32_t n, uint32_t dim, uint32_t K, const uint32_t* __restrict__ ep_dev,
-             uint32_t topm, uint32_t fd, float thre, uint32_t* __restrict__ P_ids,
-             float* __restrict__ P_dis, uint32_t* __restrict__ P_cnt) {
+             uint32_t* __restrict__ ctr, uint32_t topm, uint32_t fd, float thre,
+             uint32_t* __restrict__ P_ids, float* __restrict__ P_dis, uint32_t* __restrict__ P_cnt) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   SelLayout lay{kPath ? topm + K : 0u, kSelectCand + K, fd};
@@ -542,7 +550,7 @@ __global__ void __launch_bounds__(kWarps * 32, 8)
   Beam bm = beam_carve(reinterpret_cast<unsigned char*>(seld + fd), lay.W);
   const uint32_t L = lay.L;
   const uint32_t ep = kPath ? *ep_dev : 0u;
-  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+  for (uint32_t b = next_node(ctr, lane); b < n; b = next_node(ctr, lane)) {
     const __half* q = data + (size_t)b * dim;
     if (kPath) {
       uint32_t curr = 0;
@@ -995,6 +1003,20 @@ int check_shape(const Dev& d, uint32_t fd) {
   return TAGORE_OK;
 }
 
+// One wave of resident blocks (SMs x blocks per SM at this shared-memory
+// size), fewer when the items do not fill it.
+int resident_grid(const void* fn, int threads, size_t smem, uint32_t items_per_block,
+                  uint64_t items, int* grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  TG_CUDA(cudaGetDevice(&dev));
+  TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  TG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+  if (per_sm < 1) return fail(TAGORE_EINVAL, "kernel does not fit on an SM (%zu B shared)", smem);
+  const uint64_t need = (items + items_per_block - 1) / items_per_block;
+  *grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)sms * per_sm));
+  return TAGORE_OK;
+}
+
 int set_smem(const void* fn, size_t bytes) {
   if (bytes > 227 * 1024) return fail(TAGORE_EINVAL, "shared memory request too large (%zu)", bytes);
   TG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
@@ -1027,15 +1049,18 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   const size_t sm = lay.bytes() * kWarps;
   const void* fn = path ? (const void*)k_select<true> : (const void*)k_select<false>;
   TG_TRY(set_smem(fn, sm));
-  const int grid = grid_for(kWarps, d.n);
+  int grid = 0;
+  TG_TRY(resident_grid(fn, kWarps * 32, sm, kWarps, d.n, &grid));
+  uint32_t* ctr = ep_dev + 1;
+  TG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
   const char* sel_name = path ? "prune_select_path" : "prune_select_2hop";
   stage_begin(sel_name, s);
   if (path)
-    k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
+    k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev, ctr,
                                                  a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
   else
     k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
-                                                  a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+                                                  ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
   count_launch();
   stage_end(sel_name, s);
   TG_CUDA(cudaGetLastError());
