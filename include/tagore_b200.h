@@ -102,6 +102,20 @@ int tagore_pruning(const TagorePruneParams* p, TagoreKnnState* st, const char* i
 int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const char* mode,
                        const char* metric);
 
+/* No counterpart in the reference. Same result as tagore_pruning_cfs for
+ * mode 'path' or '2-hop' with metric 'dist' or 'angle', computed without
+ * allocating device memory: every temporary comes from one static device
+ * array of 16 MiB per device (about 20,000 points at FINAL_DEGREE 32).
+ * Graphs whose temporaries do not fit, and other mode/metric pairs, return
+ * TAGORE_EINVAL. Work goes to `stream` (a cudaStream_t; NULL is the legacy
+ * default stream) and the call returns after it has finished. Calls that
+ * overlapped on the GPU would race on the shared array; calls are serialised
+ * by a process-wide lock. The first call on a device does its set-up (module
+ * load, symbol lookup, kernel attributes) and should come before any stream
+ * capture. */
+int tagore_pruning_cfs_noalloc(const TagorePruneParams* p, TagoreKnnState* st, const char* mode,
+                               const char* metric, void* stream);
+
 /* Tagore.largeIndex(devicelist, DIM, K, cluster_num, max_points, ...)
  * (pybind.cu:298-391) for a single device (devicelist = [0]). */
 int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev);

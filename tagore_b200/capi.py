@@ -70,6 +70,8 @@ SIGNATURES = {
                                  C.c_char_p]),
     "tagore_pruning_cfs": (C.c_int, [C.POINTER(PruneParams), C.POINTER(KnnState), C.c_char_p,
                                      C.c_char_p]),
+    "tagore_pruning_cfs_noalloc": (C.c_int, [C.POINTER(PruneParams), C.POINTER(KnnState),
+                                             C.c_char_p, C.c_char_p, C.c_void_p]),
     "tagore_large_index": (C.c_int, [C.POINTER(LargeParams), C.c_void_p, C.c_int]),
     "tagore_large_merge": (C.c_int, [C.POINTER(LargeParams), C.POINTER(C.c_void_p), C.c_void_p]),
     "tagore_entry_point": (C.c_int, [C.POINTER(KnnState), C.c_uint32, C.POINTER(C.c_uint32)]),
@@ -217,6 +219,14 @@ def pruning_cfs(state, final_degree, mode, metric, topm=64, thre=1.0):
     st = state.st
     p = PruneParams(st.k, st.n, st.dim, final_degree, topm, thre)
     check(lib().tagore_pruning_cfs(C.byref(p), C.byref(st), mode.encode(), metric.encode()))
+    return st.ep
+
+
+def pruning_cfs_noalloc(state, final_degree, mode, metric, topm=64, thre=1.0, stream=None):
+    st = state.st
+    p = PruneParams(st.k, st.n, st.dim, final_degree, topm, thre)
+    check(lib().tagore_pruning_cfs_noalloc(C.byref(p), C.byref(st), mode.encode(), metric.encode(),
+                                           stream))
     return st.ep
 
 

@@ -5,6 +5,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -396,6 +397,25 @@ int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const cha
   uint32_t ep = 0;
   TG_TRY(prune_cfs(dev_of(st), a, mode, metric, &ep, s.s));
   g_times.prune_ms = t.stop(s.s);
+  st->ep = ep;
+  return TAGORE_OK;
+}
+
+// For callers that may not allocate device memory while they prune: a
+// serving process that has handed all of HBM to its own arena (resident
+// shards, caches) where a library cudaMallocAsync would fail or grow a pool
+// behind the arena's back, and code that must not synchronise the device the
+// way cudaFree can. The temporaries live in one static device array per
+// device; the lock keeps calls from overlapping on it.
+int tagore_pruning_cfs_noalloc(const TagorePruneParams* p, TagoreKnnState* st, const char* mode,
+                               const char* metric, void* stream) {
+  static std::mutex lock;
+  TG_TRY(check_prune(p, st));
+  if (!mode || !metric) return fail(TAGORE_EINVAL, "null mode/metric");
+  std::lock_guard<std::mutex> hold(lock);
+  PruneArgs a{p->final_degree, p->topm, p->thre};
+  uint32_t ep = 0;
+  TG_TRY(prune_cfs_static(dev_of(st), a, mode, metric, &ep, static_cast<cudaStream_t>(stream)));
   st->ep = ep;
   return TAGORE_OK;
 }

@@ -94,6 +94,12 @@ int prune_cfs(const Dev& d, const PruneArgs& a, const std::string& mode, const s
               uint32_t* ep_host, cudaStream_t s);
 // Individual stages, exposed for the stage-level parity tests.
 int stage_cal_ep(const Dev& d, uint32_t topm, uint32_t* ep_host, cudaStream_t s);
+// Size of the per-device static scratch of prune_cfs_static.
+constexpr size_t kStaticScratchBytes = (size_t)16 << 20;
+// prune_cfs for path|2-hop with dist|angle with every temporary carved from
+// a static device array of kStaticScratchBytes; larger graphs are rejected.
+int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
+                     const std::string& metric, uint32_t* ep_host, cudaStream_t s);
 
 // ---- kNN graph (knn.cu) ----
 struct KnnArgs {

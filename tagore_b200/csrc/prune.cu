@@ -1151,6 +1151,147 @@ int prune_index(const Dev& d, const PruneArgs& a, const std::string& type, uint3
               type.c_str());
 }
 
+// ---------------------------------------------------------------------------
+// Pruning_with_CFS for path|2-hop with dist|angle without allocating: every
+// temporary of run_dist_prune and reverse_store (the validation flag, the
+// select rows, the reverse-edge keys, CUB's temporary storage) is carved
+// from one file-scope device array. The array is per device and shared by all
+// calls on it, so calls whose GPU work overlaps would race on it; the C entry
+// point serialises its calls under a lock and returns only after the work has
+// finished.
+namespace {
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+struct Carve {
+  unsigned char* base;
+  size_t used = 0;
+  void* take(size_t bytes) {
+    void* p = base ? base + used : nullptr;
+    used += (bytes + 255) & ~(size_t)255;
+    return p;
+  }
+};
+}  // namespace
+
+int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
+                     const std::string& metric, uint32_t* ep_host, cudaStream_t s) {
+  TG_TRY(check_shape(d, a.final_degree));
+  const bool path = mode == "path";
+  if ((!path && mode != "2-hop") || (metric != "dist" && metric != "angle"))
+    return fail(TAGORE_EINVAL,
+                "without allocation only path|2-hop with dist|angle are offered (mode='%s' "
+                "metric='%s')",
+                mode.c_str(), metric.c_str());
+  const int m = metric == "angle" ? 1 : 0;
+  const uint32_t fd = a.final_degree, K = d.k;
+  if (!path && K * K < kSelectCand) return fail(TAGORE_EINVAL, "2-hop collect needs K*K >= 480");
+  if (path && (a.topm == 0 || a.topm > 256)) return fail(TAGORE_EINVAL, "TOPM must be in [1, 256]");
+  const size_t E = (size_t)d.n * fd;
+  if (E >= 0xFFFFFFFFull) return fail(TAGORE_EINVAL, "too many reverse edges (%zu)", E);
+  int end_bit = 1;
+  while (end_bit < 32 && ((uint64_t)1 << end_bit) <= d.n) ++end_bit;
+  size_t sort_tmp = 0, scan_tmp = 0;
+  TG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp, (uint32_t*)nullptr,
+                                          (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                          (uint32_t*)nullptr, (int)E, 0, end_bit, s));
+  TG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                        (int)d.n, s));
+  const size_t tmp = std::max(sort_tmp, scan_tmp);
+  // Layout: flags | select rows | reverse-edge keys | CUB temporary.
+  auto layout = [&](Carve& c, uint32_t** flags, uint32_t** P_ids, float** P_dis, uint32_t** P_cnt,
+                    uint32_t** keys, uint32_t** vals, uint32_t** keys2, uint32_t** vals2,
+                    uint32_t** deg, uint32_t** off, void** tmp_p) {
+    *flags = (uint32_t*)c.take(16);  // [0] bad id, [1] entry point, [2] node counter
+    *P_ids = (uint32_t*)c.take(E * 4);
+    *P_dis = (float*)c.take(E * 4);
+    *P_cnt = (uint32_t*)c.take((size_t)d.n * 4);
+    *keys = (uint32_t*)c.take(E * 4);
+    *vals = (uint32_t*)c.take(E * 4);
+    *keys2 = (uint32_t*)c.take(E * 4);
+    *vals2 = (uint32_t*)c.take(E * 4);
+    *deg = (uint32_t*)c.take((size_t)d.n * 4);
+    *off = (uint32_t*)c.take((size_t)d.n * 4);
+    *tmp_p = c.take(tmp);
+  };
+  uint32_t *flags, *P_ids, *P_cnt, *keys, *vals, *keys2, *vals2, *deg, *off;
+  float* P_dis;
+  void* tmp_p;
+  Carve sizing{nullptr};
+  layout(sizing, &flags, &P_ids, &P_dis, &P_cnt, &keys, &vals, &keys2, &vals2, &deg, &off, &tmp_p);
+  if (sizing.used > kStaticScratchBytes)
+    return fail(TAGORE_EINVAL,
+                "POINTS=%u FINAL_DEGREE=%u needs %zu bytes of scratch; the static scratch holds "
+                "%zu",
+                d.n, fd, sizing.used, kStaticScratchBytes);
+  void* base = nullptr;
+  TG_CUDA(cudaGetSymbolAddress(&base, g_static_scratch));
+  Carve c{static_cast<unsigned char*>(base)};
+  layout(c, &flags, &P_ids, &P_dis, &P_cnt, &keys, &vals, &keys2, &vals2, &deg, &off, &tmp_p);
+
+  // validate (as validate())
+  TG_CUDA(cudaMemsetAsync(flags, 0, 16, s));
+  const size_t cnt = (size_t)d.n * d.k;
+  k_validate<<<grid_for(256, cnt), 256, 0, s>>>(d.graph, cnt, d.n, flags);
+  count_launch();
+  TG_CUDA(cudaGetLastError());
+  uint32_t bad = 0;
+  TG_CUDA(cudaMemcpyAsync(&bad, flags, 4, cudaMemcpyDeviceToHost, s));
+  TG_CUDA(cudaStreamSynchronize(s));
+  if (bad) return fail(TAGORE_EINVAL, "graph holds an id >= POINTS (%u)", d.n);
+
+  // select (as run_dist_prune)
+  uint32_t* ep_dev = flags + 1;
+  uint32_t* ctr = flags + 2;
+  if (path) {
+    const size_t sm = beam_bytes(a.topm + K) + 64;
+    TG_TRY(set_smem((const void*)k_cal_ep, sm));
+    k_cal_ep<<<1, 32, sm, s>>>(d.graph, d.data, d.center, d.dim, K, a.topm, ep_dev);
+    count_launch();
+    TG_CUDA(cudaGetLastError());
+  }
+  SelLayout lay{path ? a.topm + K : 0u, kSelectCand + K, fd};
+  const size_t sm = lay.bytes() * kWarps;
+  const void* fn = path ? (const void*)k_select<true> : (const void*)k_select<false>;
+  TG_TRY(set_smem(fn, sm));
+  int grid = 0;
+  TG_TRY(resident_grid(fn, kWarps * 32, sm, kWarps, d.n, &grid));
+  if (path)
+    k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev, ctr,
+                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+  else
+    k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
+                                                  ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+  count_launch();
+  TG_CUDA(cudaGetLastError());
+
+  // reverse store (as reverse_store with mode 0, cap = mod = K)
+  TG_CUDA(cudaMemsetAsync(deg, 0, (size_t)d.n * 4, s));
+  k_edge_keys<<<grid_for(256, E), 256, 0, s>>>(P_ids, P_cnt, d.n, fd, keys, vals, deg);
+  count_launch();
+  TG_CUDA(cudaGetLastError());
+  size_t t1 = tmp;
+  TG_CUDA(cub::DeviceScan::ExclusiveSum(tmp_p, t1, deg, off, (int)d.n, s));
+  t1 = tmp;
+  TG_CUDA(cub::DeviceRadixSort::SortPairs(tmp_p, t1, keys, keys2, vals, vals2, (int)E, 0, end_bit,
+                                          s));
+  k_reverse_fill<0><<<grid_for(8, d.n), 256, 0, s>>>(vals2, deg, off,
+                                                     reinterpret_cast<const uint32_t*>(P_dis),
+                                                     d.n, fd, K, K, d.k, d.rgraph, d.rd, d.rnum);
+  count_launch();
+  TG_CUDA(cudaGetLastError());
+
+  // filter_reverse
+  const size_t sm2 = ((size_t)(fd + K) * 8 + (size_t)fd * 8 + 16) * kWarps;
+  TG_TRY(set_smem((const void*)k_filter_reverse, sm2));
+  k_filter_reverse<<<grid, kWarps * 32, sm2, s>>>(d.graph, d.nd, d.rgraph, d.rd, d.rnum, d.data,
+                                                  d.n, d.dim, K, fd, m, a.thre, P_ids, P_cnt);
+  count_launch();
+  TG_CUDA(cudaGetLastError());
+  if (path && ep_host) TG_CUDA(cudaMemcpyAsync(ep_host, ep_dev, 4, cudaMemcpyDeviceToHost, s));
+  TG_CUDA(cudaStreamSynchronize(s));
+  return TAGORE_OK;
+}
+
 int prune_cfs(const Dev& d, const PruneArgs& a, const std::string& mode, const std::string& metric,
               uint32_t* ep_host, cudaStream_t s) {
   TG_TRY(check_shape(d, a.final_degree));
