@@ -124,6 +124,22 @@ __device__ __forceinline__ float serial_dist(Chunk chunk) {
   return __fadd_rn(x, y);
 }
 
+// The same distance between two FP16 rows of `dim` halves (a multiple of 4)
+// by a single thread, so that the 32 lanes of a warp score 32 rows at once.
+__device__ __forceinline__ float row_dist(const __half* __restrict__ a, const __half* __restrict__ b,
+                                          uint32_t dim) {
+  const uint2* A = reinterpret_cast<const uint2*>(a);
+  const uint2* B = reinterpret_cast<const uint2*>(b);
+  if (dim == 128) return serial_dist<128>([&](int j, int w) { return __ldg((w ? B : A) + j); });
+  const uint32_t chunks = dim >> 2;
+  auto leaf = [&](int slot, float& x, float& y) {
+    for (uint32_t j = slot; j < chunks; j += 32) chunk_acc(__ldg(A + j), __ldg(B + j), x, y);
+  };
+  float x, y;
+  lane_tree<5, 0>(leaf, x, y);
+  return __fadd_rn(x, y);
+}
+
 // distance_filter (src/Tagore_src.cu:1488-1490) as nvcc compiles it, one fused
 // multiply-add, and angle_filter (:1493-1495) with IEEE-rounded operations.
 __device__ __forceinline__ bool pruned_by(int metric, float res, float dis, float cur, float thre) {

@@ -223,20 +223,6 @@ __device__ void beam_update(Beam bm, uint32_t topm, uint32_t K, int lane) {
   __syncwarp();
 }
 
-// Warms L2 (and L1) with the rows a warp is about to read: lane l covers
-// 128-byte line l of each listed row.
-__device__ __forceinline__ void prefetch_rows(const __half* data, uint32_t dim, const uint32_t* ids,
-                                              uint32_t n, int lane) {
-  const uint32_t lines = (dim * 2 + 127) / 128;
-  for (uint32_t k = 0; k < n; ++k) {
-    const uint32_t id = ids[k];
-    if (id == kInv) continue;
-    const char* row = reinterpret_cast<const char*>(data + (size_t)id * dim);
-    for (uint32_t l = lane; l < lines; l += 32)
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128 * l));
-  }
-}
-
 __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __restrict__ data,
                               uint32_t dim, uint32_t K, const __half* query, uint32_t start,
                               uint32_t topm, uint32_t iters, Beam bm, uint32_t* ring_id,
@@ -248,28 +234,17 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     bm.ex[t] = 1;
   }
   __syncwarp();
+  // Seeds: the start node's row, scored one row per lane; ring slots follow
+  // the row order.
   for (uint32_t t = lane; t < K; t += 32) {
-    bm.id[topm + t] = __ldg(G + (size_t)start * K + t);
+    const uint32_t a = __ldg(G + (size_t)start * K + t);
+    const float d = row_dist(query, data + (size_t)a * dim, dim);
+    bm.id[topm + t] = a;
     bm.ex[topm + t] = 0;
-  }
-  __syncwarp();
-  prefetch_rows(data, dim, bm.id + topm, K, lane);
-  for (uint32_t i = 0; i < K; i += 4) {
-    uint32_t ids[4];
-    float d4[4];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) ids[t] = (i + t < K) ? bm.id[topm + i + t] : kInv;
-    warp_dist4(query, data, dim, ids, d4, lane);
-    if (lane == 0) {
-#pragma unroll
-      for (int t = 0; t < 4; ++t)
-        if (i + t < K) {
-          bm.dis[topm + i + t] = d4[t];
-          if (ring_id) {
-            ring_id[(i + t) % kSelectCand] = ids[t];
-            ring_dis[(i + t) % kSelectCand] = d4[t];
-          }
-        }
+    bm.dis[topm + t] = d;
+    if (ring_id) {
+      ring_id[t % kSelectCand] = a;
+      ring_dis[t % kSelectCand] = d;
     }
   }
   __syncwarp();
@@ -343,51 +318,37 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     }
     __syncwarp();
     if (to_explore == kInv) break;
-    for (uint32_t j = lane; j < K; j += 32) {
-      const uint32_t a = __ldg(G + (size_t)to_explore * K + j);
-      const bool member = beam_has(bm, a);
-      bm.dis[topm + j] = member ? kInfDis : 0.0f;
-      bm.id[topm + j] = a;
-      bm.ex[topm + j] = 0;
-      if (!member) {  // warm L2 with the rows about to be scored
-        const char* row = reinterpret_cast<const char*>(data + (size_t)a * dim);
-        for (uint32_t l = 0; l < (dim * 2 + 127) / 128; ++l)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128 * l));
-      }
-    }
-    __syncwarp();
-    // Distances of the non-members in ascending neighbour order; that order
-    // also fixes their ring slots.
-    uint32_t pend[4];
-    int np = 0;
-    auto flush = [&]() {
-      uint32_t ids[4];
-      float d4[4];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) ids[t] = (t < np) ? bm.id[topm + pend[t]] : kInv;
-      warp_dist4(query, data, dim, ids, d4, lane);
-      if (lane == 0) {
-        for (int t = 0; t < np; ++t) {
-          bm.dis[topm + pend[t]] = d4[t];
-          if (ring_id) {
-            ring_id[(curr + t) % kSelectCand] = ids[t];
-            ring_dis[(curr + t) % kSelectCand] = d4[t];
-          }
-        }
-      }
-      curr += np;
-      np = 0;
-    };
+    // Neighbours of the explored node: members of the beam keep INF_DIS; the
+    // others are listed in ascending neighbour order (which fixes their ring
+    // slots) and scored one row per lane.
+    uint32_t* fresh_at = reinterpret_cast<uint32_t*>(bm.sb);  // K <= 128 slots
+    uint32_t nfresh = 0;
     for (uint32_t base = 0; base < K; base += 32) {
       const uint32_t j = base + lane;
-      unsigned m = __ballot_sync(kFull, j < K && bm.dis[topm + j] < 1.0f);
-      while (m) {
-        pend[np++] = base + __ffs(m) - 1;
-        m &= m - 1;
-        if (np == 4) flush();
+      bool fresh = false;
+      if (j < K) {
+        const uint32_t a = __ldg(G + (size_t)to_explore * K + j);
+        fresh = !beam_has(bm, a);
+        bm.id[topm + j] = a;
+        bm.ex[topm + j] = 0;
+        bm.dis[topm + j] = kInfDis;
+      }
+      const unsigned m = __ballot_sync(kFull, fresh);
+      if (fresh) fresh_at[nfresh + __popc(m & ((1u << lane) - 1u))] = j;
+      nfresh += __popc(m);
+    }
+    __syncwarp();
+    for (uint32_t r = lane; r < nfresh; r += 32) {
+      const uint32_t j = fresh_at[r];
+      const uint32_t a = bm.id[topm + j];
+      const float d = row_dist(query, data + (size_t)a * dim, dim);
+      bm.dis[topm + j] = d;
+      if (ring_id) {
+        ring_id[(curr + r) % kSelectCand] = a;
+        ring_dis[(curr + r) % kSelectCand] = d;
       }
     }
-    if (np) flush();
+    curr += nfresh;
     __syncwarp();
     beam_update(bm, topm, K, lane);
   }
@@ -417,8 +378,22 @@ __device__ void warp_sort_mark(uint32_t* cand, float* dis, uint32_t len, int lan
   __syncwarp();
 }
 
+// Position of the r-th (0-based) set bit of m; m has more than r set bits.
+__device__ __forceinline__ uint32_t nth_bit(unsigned m, uint32_t r) {
+  for (uint32_t i = 0; i < r; ++i) m &= m - 1u;
+  return __ffs(m) - 1;
+}
+
 // Filter stage, lazily evaluated (see file header). Returns the number of ids
 // the reference stores: one less than its selection steps (:1462, :1623).
+//
+// The lanes work through the sorted list as a queue: each takes the next live
+// candidate and tests it against the kept neighbours in order, one exact
+// thread-serial distance per step, until a rule fires or it has passed them
+// all. The earliest unresolved candidate that has passed is kept, in list
+// order; a candidate further on that had passed must then also pass the new
+// neighbour. Each candidate is thus tested against exactly the neighbours
+// kept before it, as in the sequential filter.
 __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_t len,
                                 uint32_t bid, uint32_t fd, int metric, float thre,
                                 const __half* __restrict__ data, uint32_t dim, uint32_t* sel,
@@ -440,50 +415,59 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
   }
   __syncwarp();
   uint32_t nsel = 1, last_pos = first;
-  uint32_t warmed = first;  // candidates up to here have their rows warmed
-  for (uint32_t i = first + 1; i < len && nsel < fd; ++i) {
-    // keep the next 32 positions' rows on their way into L2
-    if (i + 32 > warmed + 1 && warmed + 1 < len) {
-      const uint32_t p = warmed + 1 + lane;
-      if (p < len && cand[p] != kInv) {
-        const char* row = reinterpret_cast<const char*>(data + (size_t)cand[p] * dim);
-        for (uint32_t l = 0; l < (dim * 2 + 127) / 128; ++l)
-          asm volatile("prefetch.global.L2 [%0];" ::"l"(row + 128 * l));
+  const unsigned below = (1u << lane) - 1u;
+  // lane state: 0 idle, 1 testing against sel[s], 2 passed sel[0, nsel)
+  int st = 0;
+  uint32_t pos = kInv, c = kInv, s = 0;
+  float dc = 0.0f;
+  uint32_t next = first + 1;  // next list position to hand out
+  while (nsel < fd) {
+    unsigned idle = __ballot_sync(kFull, st == 0);
+    while (idle && next < len) {
+      const uint32_t p = next + lane;
+      const unsigned live = __ballot_sync(kFull, p < len && cand[p] != kInv);
+      const uint32_t nlive = __popc(live);
+      const uint32_t take = min(nlive, (uint32_t)__popc(idle));
+      if (st == 0) {
+        const uint32_t r = __popc(idle & below);
+        if (r < take) {
+          pos = next + nth_bit(live, r);
+          c = cand[pos];
+          dc = cdis[pos];
+          s = 0;
+          st = 1;
+        }
       }
-      warmed = min(len - 1, warmed + 32);
+      next = take == nlive ? min(len, next + 32) : next + nth_bit(live, take - 1) + 1;
+      idle = __ballot_sync(kFull, st == 0);
     }
-    const uint32_t c = cand[i];
-    if (c == kInv) continue;
-    bool dup = false;
-    for (uint32_t s0 = 0; s0 < nsel; s0 += 32) {
-      const uint32_t s = s0 + lane;
-      if (__any_sync(kFull, s < nsel && sel[s] == c)) {
-        dup = true;
-        break;
+    if (!__any_sync(kFull, st != 0)) break;
+    if (st == 1) {
+      const uint32_t q = sel[s];
+      if (q == c) {
+        st = 0;  // a repeat of a kept neighbour (:1423-1427)
+      } else {
+        const float res = row_dist(data + (size_t)q * dim, data + (size_t)c * dim, dim);
+        if (pruned_by(metric, res, dc, seld[s], thre)) st = 0;
+        else if (++s == nsel) st = 2;
       }
     }
-    if (dup) continue;
-    const float dc = cdis[i];
-    const __half* cv = data + (size_t)c * dim;
-    bool pruned = false;
-    for (uint32_t s = 0; s < nsel && !pruned; s += 4) {
-      uint32_t ids[4];
-      float r4[4];
-#pragma unroll
-      for (int t = 0; t < 4; ++t) ids[t] = (s + t < nsel) ? sel[s + t] : kInv;
-      warp_dist4(cv, data, dim, ids, r4, lane);
-#pragma unroll
-      for (int t = 0; t < 4; ++t)
-        if (!pruned && s + t < nsel) pruned = pruned_by(metric, r4[t], dc, seld[s + t], thre);
-    }
-    if (!pruned) {
-      if (lane == 0) {
+    while (true) {
+      const uint32_t key = st != 0 ? pos : kInv;
+      const uint32_t mn = __reduce_min_sync(kFull, key);
+      if (mn == kInv) break;
+      const int o = __ffs(__ballot_sync(kFull, key == mn)) - 1;
+      if (__shfl_sync(kFull, st, o) != 2) break;
+      if (lane == o) {
         sel[nsel] = c;
         seld[nsel] = dc;
+        st = 0;
       }
       __syncwarp();
       ++nsel;
-      last_pos = i;
+      last_pos = mn;
+      if (nsel == fd) break;
+      if (st == 2) st = 1;  // s == nsel - 1: test the new neighbour
     }
   }
   __syncwarp();
@@ -560,19 +544,10 @@ __global__ void __launch_bounds__(kWarps * 32, 8)
         cdis[K + i] = kInfDis;
       }
     } else {
-      for (uint32_t i = lane; i < kSelectCand; i += 32)
-        cand[K + i] = __ldg(G + (size_t)__ldg(G + (size_t)b * K + i / K) * K + i % K);
-      __syncwarp();
-      for (uint32_t i = 0; i < kSelectCand; i += 4) {
-        uint32_t ids[4];
-        float d4[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) ids[t] = cand[K + i + t];
-        warp_dist4(q, data, dim, ids, d4, lane);
-        if (lane == 0) {
-#pragma unroll
-          for (int t = 0; t < 4; ++t) cdis[K + i + t] = d4[t];
-        }
+      for (uint32_t i = lane; i < kSelectCand; i += 32) {
+        const uint32_t a = __ldg(G + (size_t)__ldg(G + (size_t)b * K + i / K) * K + i % K);
+        cand[K + i] = a;
+        cdis[K + i] = row_dist(q, data + (size_t)a * dim, dim);
       }
     }
     for (uint32_t i = lane; i < K; i += 32) {
