@@ -120,8 +120,9 @@ def recall_knn(g, half_t, samp, k=10):
                           for i, s in enumerate(samp)]))
 
 
-def index_recall(rows, ep, base, queries, half_t, k=10, L=64):
-    """recall@10 of a fixed greedy search (pool L) over the pruned rows."""
+def index_recall(rows, ep, base, queries, half_t, k=10, L=128, seed=0x5EED):
+    """recall@10 of a fixed greedy search over the pruned rows: the reference's
+    NSG search (pool L, ep's neighbours plus seeded random starts)."""
     import torch
     from oracle import oracle as orc
     n = rows.shape[0]
@@ -131,7 +132,7 @@ def index_recall(rows, ep, base, queries, half_t, k=10, L=64):
     mask = np.arange(rows.shape[1] - 1)[None, :] < deg[:, None]
     adj = rows[:, 1:][mask].astype(np.uint32)
     x = base.astype(np.float32)
-    found = orc.greedy_search(x, offs, adj, ep, queries, L, k)
+    found = orc.greedy_search(x, offs, adj, ep, queries, L, k, seed)
     xq = torch.as_tensor(queries, device=half_t.device)
     xb = torch.as_tensor(x, device=half_t.device)
     d2 = (xq * xq).sum(1, keepdim=True) + (xb * xb).sum(1)[None] - 2.0 * (xq @ xb.T)
@@ -303,11 +304,14 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms,
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f16 storage, f32 arithmetic (tcgen05 f16 screen)",
+                "dtype": "f32",
                 "data": "synthetic SIFT-like mixture (seeded, 256 components)",
                 "config": {"workload": "1M x 128 SIFT-like, GNN-Descent k=96 x10 + CFS path/dist "
                                        "1.0 degree 32 m=64", "n": n, "dim": dim, "k": K,
                            "iters": ITERS, "final_degree": FD, "topm": TOPM,
+                           "storage": "f16 base", "screen": "tcgen05 f16 Gram tiles, exact f32 "
+                                                            "re-rank of every kept pair",
+                           "index_search": "reference NSG search, L=128, seeded random starts",
                            "l2": "inputs larger than L2 (512 MB FP32 + 256 MB FP16 base)",
                            "parallelism": f"replicas x{world}"},
                 "vectors_per_s": world * n / value,

@@ -206,8 +206,14 @@ typedef struct TagoreStageStat {
 int tagore_set_profiling(int on);
 int tagore_stage_stats(TagoreStageStat* out, int max, int* count);
 
-/* Frees a device buffer this library allocated (capsule destructor). */
+/* Frees a device buffer this library allocated (capsule destructor). Like
+ * cudaFree it waits for the device's work first. */
 int tagore_device_free(void* p);
+
+/* Device memory of states and temporaries comes from a memory pool per
+ * device that keeps freed memory for the next build. This returns the
+ * current device's cached memory to the system. */
+int tagore_trim_cache(void);
 
 const char* tagore_last_error(void);
 const char* tagore_version(void);

@@ -47,7 +47,7 @@ def lib():
             "orc_prune_cfs": (C.c_int, [S, u32, u32, C.c_char_p, C.c_char_p, f32, C.POINTER(u32)]),
             "orc_host_prep": (C.c_int, [vp, u32, u32, vp, vp, C.POINTER(f32)]),
             "orc_bruteforce_knn": (C.c_int, [vp, u32, u32, vp, u32, u32, vp, vp]),
-            "orc_greedy_search": (C.c_int, [vp, u32, u32, vp, vp, u32, vp, u32, u32, u32, vp]),
+            "orc_greedy_search": (C.c_int, [vp, u32, u32, vp, vp, u32, vp, u32, u32, u32, C.c_uint64, vp]),
             "orc_nndescent": (C.c_int, [vp, u32, u32, u32, u32, u32, C.c_uint64, vp, vp]),
             "orc_num_threads": (C.c_int, []),
         }
@@ -157,14 +157,14 @@ def bruteforce_knn(base, queries, k, exclude_self=None):
     return out
 
 
-def greedy_search(base, offsets, adj, ep, queries, L, k):
+def greedy_search(base, offsets, adj, ep, queries, L, k, seed=0):
     base = np.ascontiguousarray(base, dtype=np.float32)
     q = np.ascontiguousarray(queries, dtype=np.float32)
     offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
     adj = np.ascontiguousarray(adj, dtype=np.uint32)
     out = np.empty((q.shape[0], k), np.uint32)
     lib().orc_greedy_search(_p(base), base.shape[0], base.shape[1], _p(offsets), _p(adj), ep, _p(q),
-                            q.shape[0], L, k, _p(out))
+                            q.shape[0], L, k, seed, _p(out))
     return out
 
 

@@ -771,11 +771,15 @@ int orc_bruteforce_knn(const float* base, uint32_t n, uint32_t dim, const float*
 }
 
 // Greedy best-first search over an index (the NSG search loop the reference
-// keeps as dead code, src/common.cu:65-127), with a visited bitmap, pool size
-// L, starting from `ep` and its adjacency. Adjacency is CSR (offsets, ids).
+// keeps as dead code, src/common.cu:65-127), with a visited bitmap and pool
+// size L. As there, the pool starts from ep's adjacency filled up to L with
+// random unvisited ids (:74-82); the ids come from a splitmix64 stream of
+// (seed, query index) instead of rand(), so two indexes over the same base
+// are searched from the same starts. seed == 0 starts from ep and its
+// adjacency alone. Adjacency is CSR (offsets, ids).
 int orc_greedy_search(const float* base, uint32_t n, uint32_t dim, const uint64_t* offs,
                       const uint32_t* adj, uint32_t ep, const float* q, uint32_t nq, uint32_t L,
-                      uint32_t k, uint32_t* out) {
+                      uint32_t k, uint64_t seed, uint32_t* out) {
 #pragma omp parallel
   {
     std::vector<uint8_t> seen(n);
@@ -812,8 +816,20 @@ int orc_greedy_search(const float* base, uint32_t n, uint32_t dim, const uint64_
         pool.insert(it, c);
         if (pool.size() > L) pool.pop_back();
       };
-      visit(ep);
+      if (seed == 0) visit(ep);
       for (uint64_t e = offs[ep]; e < offs[ep + 1]; ++e) visit(adj[e]);
+      if (seed != 0) {
+        uint64_t z = seed ^ (0x9E3779B97F4A7C15ull * (uint64_t)(qi + 1));
+        auto next = [&]() {
+          z += 0x9E3779B97F4A7C15ull;
+          uint64_t x = z;
+          x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+          x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+          return x ^ (x >> 31);
+        };
+        const uint32_t want = std::min<uint32_t>(L, n);
+        while (touched.size() < want) visit((uint32_t)(next() % n));
+      }
       while (true) {
         size_t idx = 0;
         while (idx < pool.size() && !pool[idx].open) ++idx;

@@ -102,6 +102,7 @@ SIGNATURES = {
     "tagore_set_profiling": (C.c_int, [C.c_int]),
     "tagore_stage_stats": (C.c_int, [C.POINTER(StageStat), C.c_int, C.POINTER(C.c_int)]),
     "tagore_device_free": (C.c_int, [C.c_void_p]),
+    "tagore_trim_cache": (C.c_int, []),
     "tagore_last_error": (C.c_char_p, []),
     "tagore_version": (C.c_char_p, []),
 }

@@ -103,6 +103,48 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
   return e == cudaErrorMemoryAllocation ? TAGORE_ENOMEM : TAGORE_ECUDA;
 }
 
+// One pool per device, created on first use, with no release threshold: a
+// build's states and scratch (several GB at 1M points) are mapped once and
+// reused by later builds instead of being unmapped at every synchronisation
+// as the default pool does.
+static std::mutex g_pool_lock;
+static cudaMemPool_t g_pools[64] = {};
+
+static int device_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  TG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(TAGORE_EINVAL, "device %d out of range", dev);
+  std::lock_guard<std::mutex> hold(g_pool_lock);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    TG_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t keep = UINT64_MAX;
+    TG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return TAGORE_OK;
+}
+
+int pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+  cudaMemPool_t pool;
+  TG_TRY(device_pool(&pool));
+  const cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, s);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return cuda_fail(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
+  }
+  return TAGORE_OK;
+}
+
+void pool_free(void* p, cudaStream_t s) {
+  if (p) cudaFreeAsync(p, s);
+}
+
 namespace {
 
 // The caller's stream (tagore_set_stream) or a non-blocking stream owned by
@@ -275,35 +317,54 @@ int tagore_state_alloc(uint32_t n, uint32_t dim, uint32_t k, TagoreKnnState* out
   out->norm_factor = 1.0f;
   out->owns = 1;
   cudaGetDevice(&out->device);
+  Stream s;
+  TG_TRY(s.init());
   for (int w = 0; w <= 8; ++w) {
     void** p = slot(out, w);
     const size_t b = buffer_bytes(n, dim, k, w);
-    cudaError_t e = cudaMalloc(p, b);
-    if (e == cudaSuccess) e = cudaMemset(*p, 0, b);
-    if (e != cudaSuccess) {
+    int rc = pool_alloc(p, b, s.s);
+    if (rc == TAGORE_OK) {
+      const cudaError_t e = cudaMemsetAsync(*p, 0, b, s.s);
+      if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemsetAsync(state)", __FILE__, __LINE__);
+    }
+    if (rc != TAGORE_OK) {
+      cudaStreamSynchronize(s.s);
       tagore_state_free(out);
-      return cuda_fail(e, "cudaMalloc(state)", __FILE__, __LINE__);
+      return rc;
     }
   }
-  TG_CUDA(cudaDeviceSynchronize());  // zero fill done before work on any stream
+  TG_CUDA(cudaStreamSynchronize(s.s));  // zero fill done before work on any stream
   return TAGORE_OK;
 }
 
+// Buffers go back to the pool once all work on the device has finished, as
+// cudaFree would wait for it.
 int tagore_device_free(void* p) {
-  if (p) TG_CUDA(cudaFree(p));
+  if (!p) return TAGORE_OK;
+  TG_CUDA(cudaDeviceSynchronize());
+  TG_CUDA(cudaFreeAsync(p, nullptr));
   return TAGORE_OK;
 }
 
 int tagore_state_free(TagoreKnnState* st) {
   if (!st) return TAGORE_OK;
   if (st->owns) {
+    cudaDeviceSynchronize();
     for (int w = 0; w <= 8; ++w) {
       void** p = slot(st, w);
-      if (*p) cudaFree(*p);
+      if (*p) cudaFreeAsync(*p, nullptr);
       *p = nullptr;
     }
   }
   st->owns = 0;
+  return TAGORE_OK;
+}
+
+int tagore_trim_cache(void) {
+  cudaMemPool_t pool;
+  TG_TRY(device_pool(&pool));
+  TG_CUDA(cudaDeviceSynchronize());
+  TG_CUDA(cudaMemPoolTrimTo(pool, 0));
   return TAGORE_OK;
 }
 
@@ -337,16 +398,15 @@ int tagore_gnn_descent_host(const TagoreKnnParams* p, const float* data, uint32_
   TG_TRY(st.init());
   TG_TRY(tagore_state_alloc(n, dim, p->k, out));
   float* raw = nullptr;
-  cudaError_t e = cudaMallocAsync((void**)&raw, (size_t)n * dim * 4, st.s);
-  if (e != cudaSuccess) {
+  int rc = pool_alloc((void**)&raw, (size_t)n * dim * 4, st.s);
+  if (rc != TAGORE_OK) {
     tagore_state_free(out);
-    return cuda_fail(e, "cudaMallocAsync(raw)", __FILE__, __LINE__);
+    return rc;
   }
-  int rc = TAGORE_OK;
-  e = cudaMemcpyAsync(raw, data, (size_t)n * dim * 4, cudaMemcpyHostToDevice, st.s);
+  const cudaError_t e = cudaMemcpyAsync(raw, data, (size_t)n * dim * 4, cudaMemcpyHostToDevice, st.s);
   if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(raw)", __FILE__, __LINE__);
   if (rc == TAGORE_OK) rc = build_from_device(p, raw, data, n, dim, out, st.s);
-  cudaFreeAsync(raw, st.s);
+  pool_free(raw, st.s);
   cudaStreamSynchronize(st.s);
   if (rc != TAGORE_OK) tagore_state_free(out);
   return rc;
@@ -403,7 +463,7 @@ int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const cha
 
 // For callers that may not allocate device memory while they prune: a
 // serving process that has handed all of HBM to its own arena (resident
-// shards, caches) where a library cudaMallocAsync would fail or grow a pool
+// shards, caches) where a library allocation would fail or grow a pool
 // behind the arena's back, and code that must not synchronise the device the
 // way cudaFree can. The temporaries live in one static device array per
 // device; the lock keeps calls from overlapping on it.

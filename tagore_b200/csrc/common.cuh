@@ -126,8 +126,10 @@ __device__ __forceinline__ float serial_dist(Chunk chunk) {
 
 // The same distance between two FP16 rows of `dim` halves (a multiple of 4)
 // by a single thread, so that the 32 lanes of a warp score 32 rows at once.
-__device__ __forceinline__ float row_dist(const __half* __restrict__ a, const __half* __restrict__ b,
-                                          uint32_t dim) {
+// Kept out of line: one copy of the unrolled 128-dim tree (about 500
+// instructions) serves every call site and stays in the instruction cache.
+static __device__ __noinline__ float row_dist(const __half* __restrict__ a,
+                                              const __half* __restrict__ b, uint32_t dim) {
   const uint2* A = reinterpret_cast<const uint2*>(a);
   const uint2* B = reinterpret_cast<const uint2*>(b);
   if (dim == 128) return serial_dist<128>([&](int j, int w) { return __ldg((w ? B : A) + j); });

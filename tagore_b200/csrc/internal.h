@@ -58,23 +58,26 @@ inline Dev dev_of(const TagoreKnnState* s) {
 }
 
 // Stream-ordered device scratch that frees itself.
+// ---- device memory (capi.cu) ----
+// States and scratch come from one memory pool per device that keeps freed
+// memory cached, so repeated builds map no new pages;
+// tagore_trim_cache() gives the cached memory back.
+int pool_alloc(void** p, size_t bytes, cudaStream_t s);
+void pool_free(void* p, cudaStream_t s);
+
+// Stream-ordered scratch from the device pool, released on the same stream.
 struct Scratch {
   cudaStream_t s;
   void* p = nullptr;
   explicit Scratch(cudaStream_t st) : s(st) {}
   int alloc(size_t bytes) {
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMallocAsync(&p, bytes, s);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      return cuda_fail(e, "cudaMallocAsync(scratch)", __FILE__, __LINE__);
-    }
-    return TAGORE_OK;
+    return pool_alloc(&p, bytes, s);
   }
   template <class T>
   T* as() const { return reinterpret_cast<T*>(p); }
   ~Scratch() {
-    if (p) cudaFreeAsync(p, s);
+    if (p) pool_free(p, s);
   }
   Scratch(const Scratch&) = delete;
   Scratch& operator=(const Scratch&) = delete;

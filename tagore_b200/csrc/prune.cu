@@ -41,16 +41,18 @@ struct Beam {
   uint8_t* ex;
   uint32_t* hash;  // membership set of the W beam ids (open addressing)
   uint32_t hmask;  // hash slots - 1
-  float* sb;       // scratch: sorted new distances (K)
-  float* sm;       // scratch: merged distances of positions 0..TOPM
+  float* sb;       // scratch (K): the fresh positions, then sorted entering distances
+  float* sm;       // staging (W + 1): merged distances of positions 0..TOPM
+  uint32_t* sid;   // staging (W + 1): their ids
+  uint8_t* sex;    // staging (W + 1): their explored flags
 };
 
 // Hash slots: a power of two holding the beam at load <= 3/4 (TOPM <= 256, K <= 128).
 __host__ __device__ inline uint32_t hash_slots(uint32_t W) { return W <= 192 ? 256u : 512u; }
 
 __host__ __device__ inline size_t beam_bytes(uint32_t W) {
-  return (size_t)hash_slots(W) * 4 + (size_t)W * 8 + ((W + 15u) & ~15u) + 128 * 4 +
-         (size_t)(W + 1) * 4;
+  return (size_t)hash_slots(W) * 4 + (size_t)W * 8 + 128 * 4 + (size_t)(W + 1) * 8 +
+         ((W + 15u) & ~15u) + ((W + 16u) & ~15u);
 }
 
 __device__ inline Beam beam_carve(unsigned char* p, uint32_t W) {
@@ -61,7 +63,9 @@ __device__ inline Beam beam_carve(unsigned char* p, uint32_t W) {
   b.dis = reinterpret_cast<float*>(b.id + W);
   b.sb = b.dis + W;
   b.sm = b.sb + 128;
-  b.ex = reinterpret_cast<uint8_t*>(b.sm + W + 1);
+  b.sid = reinterpret_cast<uint32_t*>(b.sm + W + 1);
+  b.ex = reinterpret_cast<uint8_t*>(b.sid + W + 1);
+  b.sex = b.ex + ((W + 15u) & ~15u);
   return b;
 }
 
@@ -124,103 +128,118 @@ __device__ __forceinline__ void sorted_keys(const Beam& bm, uint32_t off, uint32
 
 __device__ __forceinline__ float key_dis(uint64_t k) { return __uint_as_float((uint32_t)(k >> 32)); }
 
-// After an expansion: [0, topm) holds the previous sorted prefix, [topm, W)
-// the K new entries. The reference sorts all W with its network; only
-// [0, topm) and the set of the W ids survive into the next expansion (the
-// rest is overwritten), and with strictly increasing distances over merged
-// positions 0..topm that part is the same for every correct sort. So the new
-// entries are sorted in registers and merged into the prefix by rank; a tie
-// there falls back to the network.
-__device__ void beam_update(Beam bm, uint32_t topm, uint32_t K, int lane) {
-  const uint32_t W = topm + K;
-  if (topm > 128 || K > 128) {
-    beam_network(bm, 0, W, lane);
-    beam_rehash(bm, W, lane);
-    return;
-  }
-  beam_rehash(bm, W, lane);  // the set of all W ids, before anything moves
-  uint64_t key[4];
-  sorted_keys(bm, topm, K, key, lane);
+// Merges the m entering entries, whose (distance, slot) keys sit in sm/sid
+// [0, m), into the sorted prefix [0, topm) by rank, through the staging
+// arrays. Returns false (nothing moved) when two merged positions 0..topm tie.
+template <int E>
+__device__ bool beam_merge(Beam bm, uint32_t topm, uint32_t m, int lane) {
+  uint64_t key[E];
 #pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const uint32_t p = lane + 32 * t;
-    if (p < K) bm.sb[p] = key_dis(key[t]);
+  for (int t = 0; t < E; ++t) {
+    const uint32_t q = lane + 32 * t;
+    key[t] = q < m ? (((uint64_t)__float_as_uint(bm.sm[q]) << 32) | bm.sid[q]) : ~0ull;
+  }
+  knn::warp_sort_keys<E>(key, lane);
+#pragma unroll
+  for (int t = 0; t < E; ++t) {
+    const uint32_t q = lane + 32 * t;
+    if (q < m) bm.sb[q] = key_dis(key[t]);
   }
   __syncwarp();
-  // ranks: prefix i -> i + #(new < A_i); new p -> p + #(prefix <= B_p)
-  uint32_t ra[4], rb[4];
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const uint32_t i = lane + 32 * t;
-    ra[t] = kInv;
-    if (i < topm) {
-      const float a = bm.dis[i];
-      uint32_t lo = 0, hi = K;
-      while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (bm.sb[mid] < a) lo = mid + 1;
-        else hi = mid;
-      }
-      ra[t] = i + lo;
+  // merged rank: prefix i -> i + #(entering < A_i); entering q -> q + #(prefix <= B_q)
+  for (uint32_t i = lane; i < topm; i += 32) {
+    const float a = bm.dis[i];
+    uint32_t lo = 0, hi = m;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (bm.sb[mid] < a) lo = mid + 1;
+      else hi = mid;
     }
-    const uint32_t p = lane + 32 * t;
-    rb[t] = kInv;
-    if (p < K) {
-      const float b = key_dis(key[t]);
+    const uint32_t r = i + lo;
+    if (r <= topm) {
+      bm.sm[r] = a;
+      bm.sid[r] = bm.id[i];
+      bm.sex[r] = bm.ex[i];
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < E; ++t) {
+    const uint32_t q = lane + 32 * t;
+    if (q < m) {
+      const float v = key_dis(key[t]);
       uint32_t lo = 0, hi = topm;
       while (lo < hi) {
         const uint32_t mid = (lo + hi) >> 1;
-        if (bm.dis[mid] <= b) lo = mid + 1;
+        if (bm.dis[mid] <= v) lo = mid + 1;
         else hi = mid;
       }
-      rb[t] = p + lo;
+      const uint32_t r = q + lo;
+      if (r <= topm) {
+        const uint32_t j = (uint32_t)(key[t] & 0xFFFFFFFFu);
+        bm.sm[r] = v;
+        bm.sid[r] = bm.id[topm + j];
+        bm.sex[r] = bm.ex[topm + j];
+      }
     }
-  }
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    if (ra[t] <= topm) bm.sm[ra[t]] = bm.dis[lane + 32 * t];
-    if (rb[t] <= topm) bm.sm[rb[t]] = key_dis(key[t]);
   }
   __syncwarp();
   bool tie = false;
   for (uint32_t p = lane + 1; p <= topm; p += 32) tie |= bm.sm[p] == bm.sm[p - 1];
-  if (__any_sync(kFull, tie)) {
+  if (__any_sync(kFull, tie)) return false;
+  for (uint32_t i = lane; i < topm; i += 32) {
+    bm.dis[i] = bm.sm[i];
+    bm.id[i] = bm.sid[i];
+    bm.ex[i] = bm.sex[i];
+  }
+  __syncwarp();
+  return true;
+}
+
+// After an expansion: [0, topm) holds the previous sorted prefix, [topm, W)
+// the K new entries, of which the `nfresh` at slots fresh[0, nfresh) were
+// scored and the rest are beam members at INF_DIS. The reference sorts all W
+// with its network; only [0, topm) and the set of the W ids survive into the
+// next expansion (the rest is overwritten), and with strictly increasing
+// distances over merged positions 0..topm that part is the same for every
+// correct sort. With a full prefix only scored entries no farther than its
+// last one can reach positions 0..topm, so just those are sorted and merged
+// by rank; a tie there, or a prefix that is not full, runs the network.
+__device__ void beam_update(Beam bm, uint32_t topm, uint32_t K, const uint32_t* fresh,
+                            uint32_t nfresh, int lane) {
+  const uint32_t W = topm + K;
+  beam_rehash(bm, W, lane);  // the set of all W ids, before anything moves
+  const float worst = bm.dis[topm - 1];
+  if (topm > 128 || !(worst < kInfDis)) {
     beam_network(bm, 0, W, lane);
     return;
   }
-  // gather the survivors' payloads, then write the new prefix
-  uint32_t vid[8], vex[8];
-  float vdis[8];
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const uint32_t i = lane + 32 * t;
-    if (ra[t] < topm) {
-      vid[t] = bm.id[i];
-      vex[t] = bm.ex[i];
-      vdis[t] = bm.dis[i];
+  const unsigned below = (1u << lane) - 1u;
+  uint32_t m = 0;
+  for (uint32_t base = 0; base < nfresh; base += 32) {
+    const uint32_t r = base + lane;
+    bool enter = false;
+    float d = 0.0f;
+    uint32_t j = 0;
+    if (r < nfresh) {
+      j = fresh[r];
+      d = bm.dis[topm + j];
+      enter = d <= worst;
     }
-    if (rb[t] < topm) {
-      const uint32_t j = (uint32_t)(key[t] & 0xFFFFFFFFu);
-      vid[4 + t] = bm.id[topm + j];
-      vex[4 + t] = bm.ex[topm + j];
-      vdis[4 + t] = key_dis(key[t]);
+    const unsigned mk = __ballot_sync(kFull, enter);
+    if (enter) {
+      const uint32_t q = m + __popc(mk & below);
+      bm.sm[q] = d;
+      bm.sid[q] = j;
     }
+    m += __popc(mk);
   }
+  if (m == 0) return;  // every scored entry lies beyond the prefix: nothing moves
   __syncwarp();
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    if (ra[t] < topm) {
-      bm.id[ra[t]] = vid[t];
-      bm.ex[ra[t]] = (uint8_t)vex[t];
-      bm.dis[ra[t]] = vdis[t];
-    }
-    if (rb[t] < topm) {
-      bm.id[rb[t]] = vid[4 + t];
-      bm.ex[rb[t]] = (uint8_t)vex[4 + t];
-      bm.dis[rb[t]] = vdis[4 + t];
-    }
-  }
-  __syncwarp();
+  bool ok;
+  if (m <= 32) ok = beam_merge<1>(bm, topm, m, lane);
+  else if (m <= 64) ok = beam_merge<2>(bm, topm, m, lane);
+  else ok = beam_merge<4>(bm, topm, m, lane);
+  if (!ok) beam_network(bm, 0, W, lane);
 }
 
 __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __restrict__ data,
@@ -350,7 +369,7 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
     }
     curr += nfresh;
     __syncwarp();
-    beam_update(bm, topm, K, lane);
+    beam_update(bm, topm, K, fresh_at, nfresh, lane);
   }
   if (ring_count) *ring_count = curr;
   return bm.id[0];
@@ -397,7 +416,7 @@ __device__ __forceinline__ uint32_t nth_bit(unsigned m, uint32_t r) {
 __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_t len,
                                 uint32_t bid, uint32_t fd, int metric, float thre,
                                 const __half* __restrict__ data, uint32_t dim, uint32_t* sel,
-                                float* seld, int lane) {
+                                float* seld, int lane, uint32_t* scored = nullptr) {
   uint32_t first = kInv;
   for (uint32_t base = 0; base < len; base += 32) {
     const uint32_t i = base + lane;
@@ -414,7 +433,7 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
     seld[0] = cdis[first];
   }
   __syncwarp();
-  uint32_t nsel = 1, last_pos = first;
+  uint32_t nsel = 1, last_pos = first, rows = 0;
   const unsigned below = (1u << lane) - 1u;
   // lane state: 0 idle, 1 testing against sel[s], 2 passed sel[0, nsel)
   int st = 0;
@@ -448,6 +467,7 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
         st = 0;  // a repeat of a kept neighbour (:1423-1427)
       } else {
         const float res = row_dist(data + (size_t)q * dim, data + (size_t)c * dim, dim);
+        ++rows;
         if (pruned_by(metric, res, dc, seld[s], thre)) st = 0;
         else if (++s == nsel) st = 2;
       }
@@ -471,6 +491,7 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
     }
   }
   __syncwarp();
+  if (scored) *scored = __reduce_add_sync(kFull, rows);
   if (nsel == fd) return fd - 1;
   if (nsel >= 2 && last_pos == len - 1) return nsel - 1;
   return nsel;
@@ -518,11 +539,12 @@ __device__ __forceinline__ uint32_t next_node(uint32_t* ctr, int lane) {
 }
 
 template <bool kPath>
-__global__ void __launch_bounds__(kWarps * 32, 8)
+__global__ void __launch_bounds__(kWarps * 32, 6)
     k_select(const uint32_t* __restrict__ G, float* __restrict__ nd, const __half* __restrict__ data,
              uint32_t n, uint32_t dim, uint32_t K, const uint32_t* __restrict__ ep_dev,
              uint32_t* __restrict__ ctr, uint32_t topm, uint32_t fd, float thre,
-             uint32_t* __restrict__ P_ids, float* __restrict__ P_dis, uint32_t* __restrict__ P_cnt) {
+             uint32_t* __restrict__ P_ids, float* __restrict__ P_dis, uint32_t* __restrict__ P_cnt,
+             unsigned long long* __restrict__ work) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   SelLayout lay{kPath ? topm + K : 0u, kSelectCand + K, fd};
@@ -536,9 +558,11 @@ __global__ void __launch_bounds__(kWarps * 32, 8)
   const uint32_t ep = kPath ? *ep_dev : 0u;
   for (uint32_t b = next_node(ctr, lane); b < n; b = next_node(ctr, lane)) {
     const __half* q = data + (size_t)b * dim;
+    uint32_t scored = kSelectCand;  // rows scored for this node (2-hop: the 480 collected)
     if (kPath) {
       uint32_t curr = 0;
       warp_beam(G, data, dim, K, q, ep, topm, 10, bm, cand + K, cdis + K, &curr, lane);
+      scored = curr;
       for (uint32_t i = curr + lane; i < kSelectCand; i += 32) {
         cand[K + i] = kInv;
         cdis[K + i] = kInfDis;
@@ -556,8 +580,10 @@ __global__ void __launch_bounds__(kWarps * 32, 8)
     }
     __syncwarp();
     warp_sort_mark(cand, cdis, L, lane);
-    const uint32_t stored =
-        warp_filter(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel, seld, lane);
+    uint32_t filtered = 0;
+    const uint32_t stored = warp_filter(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel,
+                                        seld, lane, &filtered);
+    if (work && lane == 0) atomicAdd(work, (unsigned long long)(scored + filtered));
     for (uint32_t i = lane; i < stored; i += 32) {
       P_ids[(size_t)b * fd + i] = sel[i];
       P_dis[(size_t)b * fd + i] = seld[i];
@@ -1005,11 +1031,13 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   if (!path && K * K < kSelectCand) return fail(TAGORE_EINVAL, "2-hop collect needs K*K >= 480");
   if (path && (a.topm == 0 || a.topm > 256)) return fail(TAGORE_EINVAL, "TOPM must be in [1, 256]");
   Scratch sc(s);
-  TG_TRY(sc.alloc((size_t)d.n * fd * 8 + (size_t)d.n * 4 + 16));
-  uint32_t* P_ids = sc.as<uint32_t>();
+  TG_TRY(sc.alloc(16 + (size_t)d.n * fd * 8 + (size_t)d.n * 4));
+  // [u64 rows scored][u32 entry point][u32 node counter] | select rows
+  unsigned long long* work = sc.as<unsigned long long>();
+  uint32_t* ep_dev = reinterpret_cast<uint32_t*>(work + 1);
+  uint32_t* P_ids = ep_dev + 2;
   float* P_dis = reinterpret_cast<float*>(P_ids + (size_t)d.n * fd);
   uint32_t* P_cnt = reinterpret_cast<uint32_t*>(P_dis + (size_t)d.n * fd);
-  uint32_t* ep_dev = P_cnt + d.n;
   if (path) {
     const uint32_t W = a.topm + K;
     const size_t sm = beam_bytes(W) + 64;
@@ -1027,15 +1055,17 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   int grid = 0;
   TG_TRY(resident_grid(fn, kWarps * 32, sm, kWarps, d.n, &grid));
   uint32_t* ctr = ep_dev + 1;
+  TG_CUDA(cudaMemsetAsync(work, 0, 8, s));
   TG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
   const char* sel_name = path ? "prune_select_path" : "prune_select_2hop";
   stage_begin(sel_name, s);
   if (path)
     k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev, ctr,
-                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt, work);
   else
     k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
-                                                  ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+                                                  ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt,
+                                                  work);
   count_launch();
   stage_end(sel_name, s);
   TG_CUDA(cudaGetLastError());
@@ -1053,7 +1083,13 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   if (path && ep_host) {
     TG_CUDA(cudaMemcpyAsync(ep_host, ep_dev, 4, cudaMemcpyDeviceToHost, s));
   }
+  unsigned long long rows = 0;
+  if (profiling()) TG_CUDA(cudaMemcpyAsync(&rows, work, 8, cudaMemcpyDeviceToHost, s));
   TG_CUDA(cudaStreamSynchronize(s));
+  // select traffic: every scored row (2d bytes), the kNN row and distances
+  // read (8 B per slot), the selected ids and distances written (8 B each)
+  if (profiling())
+    stage_add(sel_name, rows * 2ull * d.dim + (uint64_t)d.n * (8ull * K + 8ull * fd + 4), d.n);
   return TAGORE_OK;
 }
 
@@ -1232,10 +1268,11 @@ int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
   TG_TRY(resident_grid(fn, kWarps * 32, sm, kWarps, d.n, &grid));
   if (path)
     k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev, ctr,
-                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt, nullptr);
   else
     k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
-                                                  ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt);
+                                                  ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt,
+                                                  nullptr);
   count_launch();
   TG_CUDA(cudaGetLastError());
 
