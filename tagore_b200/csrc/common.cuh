@@ -124,15 +124,71 @@ __device__ __forceinline__ float serial_dist(Chunk chunk) {
   return __fadd_rn(x, y);
 }
 
+// The 128-dim tree with 16-byte loads. At 128 dims each lane slot holds one
+// chunk, so level-1 node l is leaf l + leaf l+16 and level-2 node m is
+// level-1 m + level-1 m+8; chunks 2p and 2p+1 share a 16-byte load. Level-2
+// nodes are built in pairs (2p, 2p+1) from four loads per row and combined
+// exactly as the tree combines them.
+__device__ __forceinline__ void pair_acc(uint4 a, uint4 b, float& x0, float& y0, float& x1,
+                                         float& y1) {
+  chunk_acc(make_uint2(a.x, a.y), make_uint2(b.x, b.y), x0, y0);
+  chunk_acc(make_uint2(a.z, a.w), make_uint2(b.z, b.w), x1, y1);
+}
+
+// load(p, w) returns chunks 2p and 2p+1 of operand w as one 16-byte value.
+template <class Load16>
+__device__ __forceinline__ void level2_pair(Load16& load, int p, float (&x)[2], float (&y)[2]) {
+  // leaves 2p, 2p+1 (pair p), 2p+8.. (pair p+4), 2p+16.. (p+8), 2p+24.. (p+12)
+  float lx[4][2], ly[4][2];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    lx[q][0] = ly[q][0] = lx[q][1] = ly[q][1] = 0.0f;
+    pair_acc(load(p + 4 * q, 0), load(p + 4 * q, 1), lx[q][0], ly[q][0], lx[q][1], ly[q][1]);
+  }
+  // q indexes leaf offsets 0, 8, 16, 24: level 1 pairs (0,16) and (8,24),
+  // level 2 pairs the two results.
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const float ax = __fadd_rn(lx[0][h], lx[2][h]), ay = __fadd_rn(ly[0][h], ly[2][h]);
+    const float bx = __fadd_rn(lx[1][h], lx[3][h]), by = __fadd_rn(ly[1][h], ly[3][h]);
+    x[h] = __fadd_rn(ax, bx);
+    y[h] = __fadd_rn(ay, by);
+  }
+}
+
+template <class Load16>
+__device__ __forceinline__ float dist128_pairs(Load16 load) {
+  float x0[2], y0[2], x1[2], y1[2], x2[2], y2[2], x3[2], y3[2];
+  level2_pair(load, 0, x0, y0);  // level-2 nodes 0, 1
+  level2_pair(load, 2, x2, y2);  // 4, 5
+  level2_pair(load, 1, x1, y1);  // 2, 3
+  level2_pair(load, 3, x3, y3);  // 6, 7
+  // level 3: m + m+4; level 4: m + m+2; level 5: 0 + 1
+  const float x30 = __fadd_rn(x0[0], x2[0]), y30 = __fadd_rn(y0[0], y2[0]);
+  const float x31 = __fadd_rn(x0[1], x2[1]), y31 = __fadd_rn(y0[1], y2[1]);
+  const float x32 = __fadd_rn(x1[0], x3[0]), y32 = __fadd_rn(y1[0], y3[0]);
+  const float x33 = __fadd_rn(x1[1], x3[1]), y33 = __fadd_rn(y1[1], y3[1]);
+  const float x40 = __fadd_rn(x30, x32), y40 = __fadd_rn(y30, y32);
+  const float x41 = __fadd_rn(x31, x33), y41 = __fadd_rn(y31, y33);
+  return __fadd_rn(__fadd_rn(x40, x41), __fadd_rn(y40, y41));
+}
+
+__device__ __forceinline__ float row_dist128(const __half* __restrict__ a,
+                                             const __half* __restrict__ b) {
+  const uint4* A = reinterpret_cast<const uint4*>(a);
+  const uint4* B = reinterpret_cast<const uint4*>(b);
+  return dist128_pairs([&](int p, int w) { return __ldg((w ? B : A) + p); });
+}
+
 // The same distance between two FP16 rows of `dim` halves (a multiple of 4)
 // by a single thread, so that the 32 lanes of a warp score 32 rows at once.
-// Kept out of line: one copy of the unrolled 128-dim tree (about 500
-// instructions) serves every call site and stays in the instruction cache.
+// Kept out of line: one copy of the unrolled tree serves every call site and
+// stays in the instruction cache.
 static __device__ __noinline__ float row_dist(const __half* __restrict__ a,
                                               const __half* __restrict__ b, uint32_t dim) {
   const uint2* A = reinterpret_cast<const uint2*>(a);
   const uint2* B = reinterpret_cast<const uint2*>(b);
-  if (dim == 128) return serial_dist<128>([&](int j, int w) { return __ldg((w ? B : A) + j); });
+  if (dim == 128) return row_dist128(a, b);
   const uint32_t chunks = dim >> 2;
   auto leaf = [&](int slot, float& x, float& y) {
     for (uint32_t j = slot; j < chunks; j += 32) chunk_acc(__ldg(A + j), __ldg(B + j), x, y);

@@ -118,9 +118,17 @@ __device__ __forceinline__ uint2 tile_chunk(const Tile& t, uint32_t r, uint32_t 
   return *reinterpret_cast<const uint2*>(&t.x[blk][r][unit * 16 + half8 * 8]);
 }
 
+// Chunks 2p and 2p+1 of row r (one 16-byte unit of the swizzled tile).
+__device__ __forceinline__ uint4 tile_pair(const Tile& t, uint32_t r, uint32_t p) {
+  return *reinterpret_cast<const uint4*>(&t.x[p >> 3][r][((p & 7u) ^ (r & 7u)) * 16]);
+}
+
 // Exact reference-order FP32 distance of two tile rows, by one thread.
 template <int D>
 __device__ __forceinline__ float tile_dist(const Tile& t, uint32_t ra, uint32_t rb, uint32_t dim) {
+  if constexpr (D == 128) {
+    return dist128_pairs([&](int p, int w) { return tile_pair(t, w ? rb : ra, (uint32_t)p); });
+  }
   if constexpr (D > 0) {
     return serial_dist<D>([&](int j, int w) { return tile_chunk(t, w ? rb : ra, (uint32_t)j); });
   }
