@@ -29,23 +29,31 @@ namespace tagore {
 namespace knn {
 namespace {
 
-constexpr int kThreads = 128;
-constexpr uint32_t kTmemCols = 128;
+constexpr int kConsumers = 128;             // warps 0-3: one thread per tile row
+constexpr int kThreads = kConsumers + 32;    // warp 4: the producer
+constexpr int kStages = 3;                   // row tiles in flight
+constexpr uint32_t kTmemCols = 256;          // two 128-column accumulators
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
+constexpr uint32_t kDone = 0xFFFFFFFFu;      // stage node: the producer has finished
+constexpr float kOneMinusEps = 1.0f - 0.000244140625f;  // 1 - 2^-12, the screen's margin
 
 struct __align__(1024) Tile {
   uint8_t x[2][kMaxList][128];  // [64-half column block][row][128 B], SW128
 };
 
 struct __align__(1024) TcSmem {
-  Tile tile[2];
-  uint32_t ids[2][kMaxList];
-  float nrm[2][kMaxList];
-  float kth[2][kMaxList];
-  unsigned long long tma_bar[2];
-  unsigned long long mma_bar;
+  Tile tile[kStages];
+  uint32_t ids[kStages][kMaxList];
+  float hnrm[kStages][kMaxList];  // (1 - 2^-12) x exact squared norm
+  float kth[kStages][kMaxList];
+  uint32_t pairs[kConsumers * 4];  // kept (row << 16 | column) pairs of the node
+  uint32_t warp_pairs[kConsumers / 32];
+  unsigned long long full_bar[kStages];   // rows landed and stage filled
+  unsigned long long empty_bar[kStages];  // consumers done with the stage
+  unsigned long long mma_bar[2];          // accumulator written
   uint32_t taddr;
-  uint32_t node[2], nn[2], total[2];
+  uint32_t node[kStages], nn[kStages], total[kStages];
+  uint32_t filled, consumed;  // producer fills with rows; fills the consumers saw land
   int flag;
 };
 
@@ -128,34 +136,143 @@ template <int D>
 __device__ __forceinline__ float tile_dist(const Tile& t, uint32_t ra, uint32_t rb, uint32_t dim) {
   if constexpr (D == 128) {
     return dist128_pairs([&](int p, int w) { return tile_pair(t, w ? rb : ra, (uint32_t)p); });
-  }
-  if constexpr (D > 0) {
+  } else if constexpr (D > 0) {
     return serial_dist<D>([&](int j, int w) { return tile_chunk(t, w ? rb : ra, (uint32_t)j); });
-  }
-  float x[32], y[32];
-#pragma unroll
-  for (int l = 0; l < 32; ++l) {
-    x[l] = 0.0f;
-    y[l] = 0.0f;
-  }
-  if constexpr (D > 0) {
-#pragma unroll
-    for (int j = 0; j < D / 4; ++j) chunk_acc(tile_chunk(t, ra, j), tile_chunk(t, rb, j), x[j & 31], y[j & 31]);
   } else {
+    float x[32], y[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) {
+      x[l] = 0.0f;
+      y[l] = 0.0f;
+    }
     for (uint32_t j = 0; j < dim / 4; ++j)
       chunk_acc(tile_chunk(t, ra, j), tile_chunk(t, rb, j), x[j & 31], y[j & 31]);
-  }
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
+    for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
-    for (int l = 0; l < off; ++l) {
-      x[l] = __fadd_rn(x[l], x[l + off]);
-      y[l] = __fadd_rn(y[l], y[l + off]);
+      for (int l = 0; l < off; ++l) {
+        x[l] = __fadd_rn(x[l], x[l + off]);
+        y[l] = __fadd_rn(y[l], y[l + off]);
+      }
     }
+    return __fadd_rn(x[0], y[0]);
   }
-  return __fadd_rn(x[0], y[0]);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void consumers_sync() {
+  asm volatile("bar.sync 1, %0;" ::"n"(kConsumers) : "memory");
+}
+
+// Barrier of the consumer warps that also tells whether any of them passed
+// `v` true.
+__device__ __forceinline__ bool consumers_any(bool v) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(out)
+      : "r"(v ? 1u : 0u), "n"(kConsumers)
+      : "memory");
+  return out != 0;
+}
+
+// Producer warp: walks this block's nodes (blockIdx.x, +gridDim.x, ...),
+// skips those without a join, and fills stage j % kStages with node j: ids,
+// norms and k-th distances by the lanes, rows by TMA tile::gather4. Runs
+// kStages nodes ahead of the consumers; ends by publishing kDone.
+template <int D>
+__device__ void join_producer(TcSmem& s, const CUtensorMap& tmap, const uint64_t* __restrict__ nb,
+                              const float* __restrict__ norms, const uint32_t* __restrict__ lists,
+                              const uint32_t* __restrict__ lcnt, uint32_t n, uint32_t dim,
+                              uint32_t K, unsigned long long* n_rows) {
+  const uint32_t lane = threadIdx.x & 31u, blocks = (dim + 63) / 64;
+  uint32_t next = blockIdx.x;
+  uint32_t ph_empty[kStages] = {};
+  for (uint32_t j = 0;; ++j) {
+    const int st = (int)(j % kStages);
+    if (j >= (uint32_t)kStages) {
+      bool ok = true;
+      if (lane == 0) {
+        ok = mbar_wait_bounded(smem_u32(&s.empty_bar[st]), ph_empty[st]);
+        if (!ok) s.flag = 0;
+      }
+      ph_empty[st] ^= 1u;
+      if (!__shfl_sync(kFull, ok ? 1 : 0, 0)) return;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    // next node with a join: 32 candidates per step, one per lane
+    uint32_t u = kDone, nn = 0, tot = 0;
+    while (next < n) {
+      const uint32_t c = next + lane * gridDim.x;
+      uint2 cnt = make_uint2(0, 0);
+      if (c < n) cnt = *reinterpret_cast<const uint2*>(lcnt + 2 * (size_t)c);
+      const unsigned ok = __ballot_sync(kFull, c < n && cnt.x > 0 && cnt.y >= 2);
+      if (ok) {
+        const int w = __ffs(ok) - 1;
+        u = next + (uint32_t)w * gridDim.x;
+        nn = __shfl_sync(kFull, cnt.x, w);
+        tot = __shfl_sync(kFull, cnt.y, w);
+        next = u + gridDim.x;
+        break;
+      }
+      next += 32u * gridDim.x;
+    }
+    if (lane == 0) {
+      s.node[st] = u;
+      s.nn[st] = nn;
+      s.total[st] = tot;
+    }
+    if (u == kDone) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&s.full_bar[st]));
+      return;
+    }
+    for (uint32_t t = lane; t < tot; t += 32) {
+      const uint32_t id = lists[(size_t)u * kMaxList + t];
+      s.ids[st][t] = id;
+      s.hnrm[st][t] = kOneMinusEps * norms[id];
+      s.kth[st][t] = kth_of(nb[(size_t)id * K + K - 1]);
+    }
+    __syncwarp();
+    const uint32_t groups = (tot + 3) / 4, bar = smem_u32(&s.full_bar[st]);
+    if (lane == 0) {
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                   "r"(groups * 4 * 128 * blocks)
+                   : "memory");
+      *n_rows += tot;
+      s.filled = j + 1;
+    }
+    __syncwarp();
+    for (uint32_t g = lane; g < groups; g += 32) {
+      uint32_t r[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) r[t] = s.ids[st][min(4 * g + t, tot - 1)];
+      for (uint32_t b = 0; b < blocks; ++b) {
+        const uint32_t dst = smem_u32(&s.tile[st].x[b][4 * g][0]);
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::"
+            "bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+            "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(b * 64), "r"(r[0]), "r"(r[1]), "r"(r[2]),
+            "r"(r[3]), "r"(bar)
+            : "memory");
+      }
+    }
+  }
+}
+
+// Warp-specialised persistent join. The producer warp (join_producer) keeps
+// kStages nodes in flight; the four consumer warps take node i from stage
+// i % kStages: thread 0 has issued its Gram tile X X^T (tcgen05, M = N = 128,
+// K = 16 steps) into accumulator i % 2 one node earlier; every thread owns
+// one tile row, screens it from TMEM and re-ranks the kept pairs exactly.
+// Blocks of at most 114 KB of shared memory run at most two per SM, so their
+// 2 x 256 TMEM columns always fit.
 template <int D>
 __global__ void __launch_bounds__(kThreads, 1)
     k_join_tc(const __grid_constant__ CUtensorMap tmap, const uint64_t* __restrict__ nb,
@@ -166,8 +283,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   extern __shared__ unsigned char smem_raw[];
   TcSmem& s = *reinterpret_cast<TcSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
-  const uint32_t mma_bar = smem_u32(&s.mma_bar);
-  const uint32_t ksteps = dim / 16, blocks = (dim + 63) / 64;
+  const uint32_t ksteps = dim / 16;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -176,189 +292,172 @@ __global__ void __launch_bounds__(kThreads, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.tma_bar[0])));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.tma_bar[1])));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mma_bar));
+    for (int st = 0; st < kStages; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.full_bar[st])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&s.empty_bar[st])));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mma_bar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mma_bar[1])));
     asm volatile("fence.mbarrier_init.release.cluster;");
     asm volatile("fence.proxy.async.shared::cta;");
     s.flag = 1;
+    s.filled = 0;
+    s.consumed = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = s.taddr;
-  uint32_t ph_tma[2] = {0, 0}, ph_mma = 0;
   unsigned long long n_pairs = 0, n_props = 0, n_rows = 0;
 
-  // Finds this block's next joinable node at or after u into stage st, loads
-  // its ids, starts its row copies and loads its norms and k-th distances.
-  // Returns false at the end of the block's share.
-  auto fetch = [&](uint32_t u, int st) -> bool {
-    if (tid == 0) {
-      uint32_t nn = 0, tot = 0;
-      while (u < n) {
-        nn = lcnt[2 * u];
-        tot = lcnt[2 * u + 1];
-        if (nn > 0 && tot >= 2) break;
-        u += gridDim.x;
-      }
-      s.node[st] = u;
-      s.nn[st] = nn;
-      s.total[st] = tot;
-    }
-    __syncthreads();
-    const uint32_t u2 = s.node[st], tot = s.total[st];
-    if (u2 >= n) return false;
-    if (tid < tot) s.ids[st][tid] = lists[(size_t)u2 * kMaxList + tid];
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      const uint32_t groups = (tot + 3) / 4, bar = smem_u32(&s.tma_bar[st]);
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                   "r"(groups * 4 * 128 * blocks)
-                   : "memory");
-      for (uint32_t g = 0; g < groups; ++g) {
-        uint32_t r[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) r[t] = s.ids[st][min(4 * g + t, tot - 1)];
-        for (uint32_t b = 0; b < blocks; ++b) {
-          const uint32_t dst = smem_u32(&s.tile[st].x[b][4 * g][0]);
-          asm volatile(
-              "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::"
-              "bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
-              "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(b * 64), "r"(r[0]), "r"(r[1]), "r"(r[2]),
-              "r"(r[3]), "r"(bar)
-              : "memory");
-        }
-      }
-      n_rows += tot;
-    }
-    if (tid < tot) {
-      const uint32_t id = s.ids[st][tid];
-      s.nrm[st][tid] = norms[id];
-      s.kth[st][tid] = kth_of(nb[(size_t)id * K + K - 1]);
-    }
-    return true;
-  };
-
-  // Waits for stage st's rows (thread 0, bounded) and issues its MMAs.
-  auto mma = [&](int st) {
-    if (tid == 0) {
-      if (!mbar_wait_bounded(smem_u32(&s.tma_bar[st]), ph_tma[st])) {
+  if (warp == kConsumers / 32) {
+    join_producer<D>(s, tmap, nb, norms, lists, lcnt, n, dim, K, &n_rows);
+  } else {
+    uint32_t ph_full[kStages] = {}, ph_mma[2] = {0, 0};
+    bool pending[2] = {false, false};  // thread 0: committed MMAs not yet waited for
+    // Thread 0: waits for stage st's rows (phase ph) and issues their Gram
+    // tile into accumulator acc. No MMA for a kDone stage or on timeout.
+    auto issue = [&](int st, uint32_t ph, uint32_t acc) {
+      if (!mbar_wait_bounded(smem_u32(&s.full_bar[st]), ph)) {
         s.flag = 0;
         return;
       }
+      if (s.node[st] == kDone) return;
       asm volatile("tcgen05.fence::after_thread_sync;");
       for (uint32_t k = 0; k < ksteps; ++k) {
         const uint64_t desc = sw128_desc(smem_u32(&s.tile[st].x[k >> 2][0][0]) + (k & 3u) * 32);
-        const uint32_t acc = k > 0 ? 1u : 0u;
+        const uint32_t accum = k > 0 ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
             "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-            "l"(desc), "l"(desc), "r"(kIdesc), "r"(acc));
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + acc * 128),
+            "l"(desc), "l"(desc), "r"(kIdesc), "r"(accum));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          mma_bar));
-    }
-  };
-
-  int cur = 0;
-  bool have = fetch(blockIdx.x, 0);
-  __syncthreads();
-  if (have) mma(0);
-  __syncthreads();
-  bool failed = s.flag == 0;
-  while (have && !failed) {
-    const int nxt = cur ^ 1;
-    const uint32_t u = s.node[cur], nn = s.nn[cur], total = s.total[cur];
-    // next node's rows go in flight while this one is finished
-    const bool have_next = fetch(u + gridDim.x, nxt);
-    // ---- Gram tile of the current node ----
-    if (tid == 0 && s.flag) s.flag = mbar_wait_bounded(mma_bar, ph_mma) ? 1 : 0;
-    __syncthreads();
-    if (!s.flag) {
-      failed = true;
-      break;
-    }
-    mbar_try(mma_bar, ph_mma);
-    mbar_try(smem_u32(&s.tma_bar[cur]), ph_tma[cur]);
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    ph_mma ^= 1u;
-    ph_tma[cur] ^= 1u;
-    // ---- screen: each thread owns one row ----
-    // Pair (r, c) may beat row r's k-th entry only if its screened distance
-    // nr + nc - 2g is below thr + eps (nr + nc), i.e. hc - 2g < thr - (1-eps) nr
-    // with hc = (1-eps) nc (eps = 2^-12). Candidates are ranked by hc - 2g.
-    const uint32_t r = tid;
-    const bool live = r < total;
-    const float one_m = 1.0f - 0.000244140625f;
-    const float lim = live ? s.kth[cur][r] - one_m * s.nrm[cur][r] : -INFINITY;
-    float bd[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
-    uint32_t bc[4] = {kInv, kInv, kInv, kInv};
+          smem_u32(&s.mma_bar[acc])));
+      pending[acc] = true;
+    };
+    if (tid == 0) issue(0, 0, 0);
+    const uint32_t r = tid, lane = tid & 31u;
+    uint32_t got_full = 0;  // nodes whose rows this thread has seen land
+    for (uint32_t i = 0;; ++i) {
+      const int st = (int)(i % kStages);
+      const uint32_t acc = i & 1u;
+      const bool got = mbar_wait_bounded(smem_u32(&s.full_bar[st]), ph_full[st]);
+      ph_full[st] ^= 1u;
+      got_full += got ? 1u : 0u;
+      const bool done = got && s.node[st] == kDone;
+      bool ok = got;
+      if (got && !done) {
+        ok = mbar_wait_bounded(smem_u32(&s.mma_bar[acc]), ph_mma[acc]);
+        ph_mma[acc] ^= 1u;
+        pending[acc] = false;
+      }
+      // every consumer leaves together: on any thread's timeout, or at kDone
+      if (consumers_any(!ok)) {
+        if (tid == 0) s.flag = 0;
+        break;
+      }
+      if (done) break;
+      const uint32_t nn = s.nn[st], total = s.total[st];
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      // ---- screen: each thread owns one row ----
+      // Pair (r, c) may beat row r's k-th entry only if its screened distance
+      // nr + nc - 2g is below thr + eps (nr + nc), i.e. hc - 2g < thr - (1-eps) nr
+      // with hc = (1-eps) nc (eps = 2^-12). Candidates are ranked by hc - 2g.
+      const bool live = r < total;
+      const float lim = live ? s.kth[st][r] - s.hnrm[st][r] : -INFINITY;
+      float bd[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+      uint32_t bc[4] = {kInv, kInv, kInv, kInv};
 #pragma unroll
-    for (int t = 0; t < 4; ++t)
-      if ((uint32_t)t >= T) bd[t] = -INFINITY;  // unused slots never accept
-    // columns a row may pair with: all others if r is new, new ones if old
-    const uint32_t cmax = (r < nn) ? total : nn;
+      for (int t = 0; t < 4; ++t)
+        if ((uint32_t)t >= T) bd[t] = -INFINITY;  // unused slots never accept
+      // columns a row may pair with: all others if r is new, new ones if old;
+      // the warp reads only the column blocks one of its rows needs
+      const uint32_t cmax = live ? ((r < nn) ? total : nn) : 0u;
+      const uint32_t wmax = __reduce_max_sync(kFull, cmax);
 #pragma unroll 1
-    for (uint32_t q = 0; q < 4; ++q) {
-      float g[32];
-      tmem_ld32(tmem + ((warp * 32u) << 16) + q * 32u, g);
+      for (uint32_t q = 0; q * 32 < wmax; ++q) {
+        float g[32];
+        tmem_ld32(tmem + acc * 128 + ((warp * 32u) << 16) + q * 32u, g);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        const uint32_t c = q * 32 + i;
-        const float v0 = fmaf(-2.0f, g[i], one_m * s.nrm[cur][c]);
-        const float worst = T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3]));
-        if (v0 < lim && v0 < worst && c < cmax && c != r) {
-          float v = v0;
-          uint32_t vc = c;
+        for (int k = 0; k < 32; ++k) {
+          const uint32_t c = q * 32 + k;
+          const float v0 = fmaf(-2.0f, g[k], s.hnrm[st][c]);
+          const float worst = T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3]));
+          if (v0 < lim && v0 < worst && c < cmax && c != r) {
+            float v = v0;
+            uint32_t vc = c;
 #pragma unroll
-          for (int t = 0; t < 4; ++t)
-            if (v < bd[t]) {
-              swap_(v, bd[t]);
-              swap_(vc, bc[t]);
-            }
+            for (int t = 0; t < 4; ++t)
+              if (v < bd[t]) {
+                swap_(v, bd[t]);
+                swap_(vc, bc[t]);
+              }
+          }
         }
       }
-    }
-    // TMEM is free: start the next node's MMA (its rows are likely in already)
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    __syncthreads();
-    if (have_next) mma(nxt);
-    // ---- exact re-rank of the kept pairs, thread per row ----
-    if (live) {
-      const uint32_t a = s.ids[cur][r];
-      const float thr = s.kth[cur][r];
+      // kept pairs go to one list so that the exact re-rank is shared evenly
+      uint32_t kept = 0;
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        if (bc[t] == kInv) continue;  // unused and empty slots
-        const float d = tile_dist<D>(s.tile[cur], r, bc[t], dim);
+      for (int t = 0; t < 4; ++t) kept += bc[t] != kInv ? 1u : 0u;
+      uint32_t incl = kept;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+      }
+      if (lane == 31) s.warp_pairs[warp] = incl;
+      // accumulator acc ^ 1 was last read for node i - 1: node i + 1 may go in
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      consumers_sync();
+      if (tid == 0) {
+        const int st1 = (int)((i + 1) % kStages);
+        issue(st1, ph_full[st1], acc ^ 1u);  // the phase node i + 1 completes
+      }
+      uint32_t off = incl - kept, npairs = 0;
+#pragma unroll
+      for (int w = 0; w < kConsumers / 32; ++w) {
+        const uint32_t c = s.warp_pairs[w];
+        if ((uint32_t)w < warp) off += c;
+        npairs += c;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if (bc[t] != kInv) s.pairs[off++] = (r << 16) | bc[t];
+      consumers_sync();
+      // ---- exact re-rank of the kept pairs ----
+      for (uint32_t q = tid; q < npairs; q += kConsumers) {
+        const uint32_t pr = s.pairs[q], row = pr >> 16, col = pr & 0xFFFFu;
+        const float d = tile_dist<D>(s.tile[st], row, col, dim);
         ++n_pairs;
-        if (d < thr) {
-          propose(pool, a, P, s.ids[cur][bc[t]], d);
+        if (d < s.kth[st][row]) {
+          propose(pool, s.ids[st][row], P, s.ids[st][col], d);
           ++n_props;
         }
       }
+      __syncwarp();
+      if ((tid & 31u) == 0) mbar_arrive(smem_u32(&s.empty_bar[st]));
     }
-    __syncthreads();
-    have = have_next;
-    cur = nxt;
-    failed = s.flag == 0;
-  }
-  if (failed) {
     if (tid == 0) {
-      atomicExch(err, 1);
-      // let this block's own copies and MMAs land before TMEM is released
-      mbar_wait_bounded(smem_u32(&s.tma_bar[0]), ph_tma[0]);
-      mbar_wait_bounded(smem_u32(&s.tma_bar[1]), ph_tma[1]);
-      mbar_wait_bounded(mma_bar, ph_mma);
+      // MMAs committed but not consumed (only after a timeout) land first
+      for (int a = 0; a < 2; ++a)
+        if (pending[a]) mbar_wait_bounded(smem_u32(&s.mma_bar[a]), ph_mma[a]);
+      s.consumed = got_full;
     }
-    __syncthreads();
   }
+  __syncthreads();
+  if (tid == 0 && !s.flag) {
+    // after a timeout, row copies the consumers never waited for land before
+    // the block's shared memory is released (at most kStages of them)
+    for (uint32_t j = s.consumed; j < s.filled; ++j)
+      mbar_wait_bounded(smem_u32(&s.full_bar[j % kStages]), (j / kStages) & 1u);
+  }
+  __syncthreads();
+  if (!s.flag && tid == 0) atomicExch(err, 1);
   if (n_props) atomicAdd(&stats[0], n_props);
   if (n_pairs) atomicAdd(&stats[1], n_pairs);
-  if (tid == 0) atomicAdd(&stats[3], n_rows);
+  if (n_rows) atomicAdd(&stats[3], n_rows);
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 0)
@@ -394,16 +493,16 @@ int make_row_map(CUtensorMap* map, const __half* base, uint32_t n, uint32_t dim)
 
 template <int D>
 int launch(const Work& w, const CUtensorMap& map, cudaStream_t s) {
-  // At least 72 KB of shared memory per block caps residency at three blocks
-  // per SM, so their 3 x 128 TMEM columns always fit.
-  const size_t sm = std::max<size_t>(sizeof(TcSmem) + 1024, 72 * 1024);
+  // More than a third of an SM's shared memory per block keeps residency at
+  // two blocks per SM, so their 2 x 256 TMEM columns always fit.
+  const size_t sm = std::max<size_t>(sizeof(TcSmem) + 1024, 80 * 1024);
   TG_CUDA(cudaFuncSetAttribute((const void*)k_join_tc<D>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int* err = reinterpret_cast<int*>(w.stats + 4);
-  k_join_tc<D><<<sms * 3, kThreads, sm, s>>>(map, w.nb, w.norms, w.lists, w.lcnt, w.n, w.dim,
+  k_join_tc<D><<<sms * 2, kThreads, sm, s>>>(map, w.nb, w.norms, w.lists, w.lcnt, w.n, w.dim,
                                              w.K, w.T, w.P, w.pool, w.stats, err);
   TG_CUDA(cudaGetLastError());
   return TAGORE_OK;
