@@ -24,7 +24,15 @@ enum {
   TAGORE_ETIMEOUT = 5  /* a bounded wait ran out */
 };
 
-enum { TAGORE_KNN_CHOSEN = 0, TAGORE_KNN_PLAIN = 1 };
+/* kNN join modes. CHOSEN: tensor-core screen + exact re-rank where the row
+ * width allows (16..128 dims in steps of 16), the learned screen otherwise;
+ * PLAIN: every pair in exact FP32; LEARNED: the learned screen at any width. */
+enum { TAGORE_KNN_CHOSEN = 0, TAGORE_KNN_PLAIN = 1, TAGORE_KNN_LEARNED = 2 };
+
+/* learn_flags of TagoreKnnParams (for measuring the screen against itself):
+ * FIXED_T keeps the per-row count instead of steering it by the miss rate;
+ * NO_TRAIN screens with the untrained start weights. */
+enum { TAGORE_LEARN_FIXED_T = 1, TAGORE_LEARN_NO_TRAIN = 2 };
 
 /* The reference's eight device buffers in its capsule order
  * (pybind.cu:132-141), plus project buffers. Ownership: created by
@@ -57,6 +65,8 @@ typedef struct TagoreKnnParams {
   uint32_t per_row;  /* proposals kept per local-join row (0: default) */
   uint32_t rescale;  /* 1: power-of-ten rescale as GNN_descent; 0: none (largeIndex) */
   uint64_t seed;
+  uint32_t learn_steps;  /* training steps of the learned screen (0: 400) */
+  uint32_t learn_flags;  /* TAGORE_LEARN_* */
 } TagoreKnnParams;
 
 typedef struct TagorePruneParams {
@@ -205,6 +215,26 @@ typedef struct TagoreStageStat {
 } TagoreStageStat;
 int tagore_set_profiling(int on);
 int tagore_stage_stats(TagoreStageStat* out, int max, int* count);
+
+/* The learned screen in the last kNN build on this thread: whether it ran,
+ * its training steps and loss on the first and last batch, how many
+ * iterations it screened, its final per-row count, the miss rate measured on
+ * sampled nodes in its last iteration (improving pairs it did not keep) and
+ * whether it handed over to the exact join. No counterpart in the reference. */
+typedef struct TagoreScreenStats {
+  uint32_t used, steps, screened_iters, per_row, fallback, pad_;
+  float loss_first, loss_last;
+  double last_miss;
+  double last_best_kept; /* share of each sampled row's exact best per_row candidates kept */
+} TagoreScreenStats;
+int tagore_last_screen(TagoreScreenStats* out);
+
+/* Loss and parameter gradients of the screen MLP on a batch, for checking the
+ * kernels: rows (n x dim FP16, host), triplets tri (3B row indices a p m,
+ * host), params (host, the layout [W1 dim x 128 | b1 128 | W2 128 x 32 | b2
+ * 32], FP32); grads receives the same layout. No counterpart in the reference. */
+int tagore_mlp_loss_grad(const uint16_t* rows, uint32_t n, uint32_t dim, const uint32_t* tri,
+                         uint32_t B, const float* params, float* grads, double* loss);
 
 /* Frees a device buffer this library allocated (capsule destructor). Like
  * cudaFree it waits for the device's work first. */

@@ -13,7 +13,8 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtagore_b200.so")
 
 TAGORE_OK, TAGORE_EINVAL, TAGORE_EIO, TAGORE_ENOMEM, TAGORE_ECUDA, TAGORE_ETIMEOUT = range(6)
-KNN_CHOSEN, KNN_PLAIN = 0, 1
+KNN_CHOSEN, KNN_PLAIN, KNN_LEARNED = 0, 1, 2
+LEARN_FIXED_T, LEARN_NO_TRAIN = 1, 2
 
 # Buffer index -> (name, numpy dtype); the reference's capsule order.
 BUFFERS = [("graph", np.uint32), ("reverse_graph", np.uint32), ("data", np.float16),
@@ -34,7 +35,8 @@ class KnnState(C.Structure):
 class KnnParams(C.Structure):
     _fields_ = [("k", C.c_uint32), ("n", C.c_uint32), ("dim", C.c_uint32), ("iters", C.c_uint32),
                 ("mode", C.c_uint32), ("sample", C.c_uint32), ("per_row", C.c_uint32),
-                ("rescale", C.c_uint32), ("seed", C.c_uint64)]
+                ("rescale", C.c_uint32), ("seed", C.c_uint64), ("learn_steps", C.c_uint32),
+                ("learn_flags", C.c_uint32)]
 
 
 class PruneParams(C.Structure):
@@ -54,6 +56,13 @@ class LargeParams(C.Structure):
 class Timings(C.Structure):
     _fields_ = [("knn_ms", C.c_double), ("prune_ms", C.c_double), ("prep_ms", C.c_double),
                 ("total_ms", C.c_double), ("kernel_launches", C.c_uint64)]
+
+
+class ScreenStats(C.Structure):
+    _fields_ = [("used", C.c_uint32), ("steps", C.c_uint32), ("screened_iters", C.c_uint32),
+                ("per_row", C.c_uint32), ("fallback", C.c_uint32), ("pad_", C.c_uint32),
+                ("loss_first", C.c_float), ("loss_last", C.c_float), ("last_miss", C.c_double),
+                ("last_best_kept", C.c_double)]
 
 
 class StageStat(C.Structure):
@@ -103,6 +112,9 @@ SIGNATURES = {
     "tagore_stage_stats": (C.c_int, [C.POINTER(StageStat), C.c_int, C.POINTER(C.c_int)]),
     "tagore_device_free": (C.c_int, [C.c_void_p]),
     "tagore_trim_cache": (C.c_int, []),
+    "tagore_last_screen": (C.c_int, [C.POINTER(ScreenStats)]),
+    "tagore_mlp_loss_grad": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
+                                       C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
     "tagore_last_error": (C.c_char_p, []),
     "tagore_version": (C.c_char_p, []),
 }
@@ -195,14 +207,17 @@ class State:
             pass
 
 
-def knn_params(k, n, dim, iters, mode=KNN_CHOSEN, sample=0, per_row=0, rescale=1, seed=0x7A6E):
-    return KnnParams(k, n, dim, iters, mode, sample, per_row, rescale, seed)
+def knn_params(k, n, dim, iters, mode=KNN_CHOSEN, sample=0, per_row=0, rescale=1, seed=0x7A6E,
+               learn_steps=0, learn_flags=0):
+    return KnnParams(k, n, dim, iters, mode, sample, per_row, rescale, seed, learn_steps,
+                     learn_flags)
 
 
-def gnn_descent_host(data, k, iters, mode=KNN_CHOSEN, rescale=1, seed=0x7A6E, sample=0, per_row=0):
+def gnn_descent_host(data, k, iters, mode=KNN_CHOSEN, rescale=1, seed=0x7A6E, sample=0, per_row=0,
+                     learn_steps=0, learn_flags=0):
     data = np.ascontiguousarray(data, dtype=np.float32)
     n, dim = data.shape
-    p = knn_params(k, n, dim, iters, mode, sample, per_row, rescale, seed)
+    p = knn_params(k, n, dim, iters, mode, sample, per_row, rescale, seed, learn_steps, learn_flags)
     s = State()
     check(lib().tagore_gnn_descent_host(C.byref(p), _ptr(data), n, dim, C.byref(s.st)))
     return s
@@ -248,6 +263,25 @@ def build_index_host(data, k, iters, final_degree, topm=64, thre=1.0, mode=KNN_C
     check(lib().tagore_build_index_host(C.byref(p), _ptr(data), n, dim, final_degree, topm, thre,
                                         _ptr(out), C.byref(ep)))
     return out, ep.value
+
+
+def last_screen():
+    t = ScreenStats()
+    check(lib().tagore_last_screen(C.byref(t)))
+    return t
+
+
+def mlp_loss_grad(rows_f16, tri, params):
+    """Loss and gradients of the screen MLP on the GPU (host arrays in and out)."""
+    rows_f16 = np.ascontiguousarray(rows_f16, dtype=np.float16)
+    n, dim = rows_f16.shape
+    tri = np.ascontiguousarray(tri, dtype=np.uint32)
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    grads = np.zeros_like(params)
+    loss = C.c_double(0.0)
+    check(lib().tagore_mlp_loss_grad(_ptr(rows_f16), n, dim, _ptr(tri), tri.shape[0],
+                                     _ptr(params), _ptr(grads), C.byref(loss)))
+    return loss.value, grads
 
 
 def last_timings():

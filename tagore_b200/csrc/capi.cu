@@ -11,12 +11,16 @@
 #include <vector>
 
 #include "internal.h"
+#include "mlp.cuh"
 
 namespace tagore {
 
 static thread_local std::string g_err;
 static thread_local TagoreTimings g_times{};
 static thread_local cudaStream_t g_user_stream = nullptr;
+static thread_local ScreenStats g_screen{};
+
+void set_screen_stats(const ScreenStats& s) { g_screen = s; }
 static std::atomic<uint64_t> g_launches{0};
 
 // ---- stage timing ----
@@ -245,7 +249,8 @@ int build_from_device(const TagoreKnnParams* p, const float* raw_dev, const floa
   TG_TRY(prep_base(raw_dev, n, dim, st->norm_factor, (__half*)st->data, (float*)st->norms, s));
   std::vector<uint16_t> center(dim);
   std::thread cth(host_center, host_for_center, n, dim, st->norm_factor, center.data());
-  KnnArgs a{p->k, p->iters, p->mode, p->sample, p->per_row, p->seed};
+  KnnArgs a{p->k,       p->iters, p->mode,        p->sample,
+            p->per_row, p->seed,  p->learn_steps, p->learn_flags};
   KnnStats ks{};
   const auto w0 = std::chrono::steady_clock::now();
   const int rc = knn_build(dev_of(st), (const float*)st->norms, a, &ks, s);
@@ -357,6 +362,43 @@ int tagore_state_free(TagoreKnnState* st) {
     }
   }
   st->owns = 0;
+  return TAGORE_OK;
+}
+
+int tagore_last_screen(TagoreScreenStats* out) {
+  if (!out) return fail(TAGORE_EINVAL, "null stats");
+  std::memset(out, 0, sizeof(*out));
+  out->used = g_screen.used;
+  out->steps = g_screen.steps;
+  out->screened_iters = g_screen.screened_iters;
+  out->per_row = g_screen.per_row;
+  out->fallback = g_screen.fallback;
+  out->loss_first = g_screen.loss_first;
+  out->loss_last = g_screen.loss_last;
+  out->last_miss = g_screen.last_miss;
+  out->last_best_kept = g_screen.last_best_kept;
+  return TAGORE_OK;
+}
+
+int tagore_mlp_loss_grad(const uint16_t* rows, uint32_t n, uint32_t dim, const uint32_t* tri,
+                         uint32_t B, const float* params, float* grads, double* loss) {
+  if (!rows || !tri || !params || !grads || !loss || n == 0 || B == 0 || dim == 0)
+    return fail(TAGORE_EINVAL, "bad screen-gradient arguments");
+  for (size_t i = 0; i < (size_t)3 * B; ++i)
+    if (tri[i] >= n) return fail(TAGORE_EINVAL, "triplet row %u >= %u", tri[i], n);
+  Stream s;
+  TG_TRY(s.init());
+  Scratch dev(s.s), work(s.s);
+  TG_TRY(dev.alloc((size_t)n * dim * 2 + (size_t)3 * B * 4 + 16));
+  __half* x = dev.as<__half>();
+  uint32_t* t = reinterpret_cast<uint32_t*>(x + (size_t)n * dim + ((size_t)n * dim & 1));
+  TG_CUDA(cudaMemcpyAsync(x, rows, (size_t)n * dim * 2, cudaMemcpyHostToDevice, s.s));
+  TG_CUDA(cudaMemcpyAsync(t, tri, (size_t)3 * B * 4, cudaMemcpyHostToDevice, s.s));
+  mlp::Net net;
+  TG_TRY(net.init(dim, 1, s.s));
+  TG_TRY(net.set_params(params, s.s));
+  TG_TRY(net.loss_grad(t, B, x, work, loss, s.s));
+  TG_TRY(net.get(nullptr, grads, s.s));
   return TAGORE_OK;
 }
 

@@ -106,11 +106,21 @@ int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
 
 // ---- kNN graph (knn.cu) ----
 struct KnnArgs {
-  uint32_t k, iters, mode;  // mode: TAGORE_KNN_CHOSEN / TAGORE_KNN_PLAIN
+  uint32_t k, iters, mode;  // mode: TAGORE_KNN_CHOSEN / _PLAIN / _LEARNED
   uint32_t sample;          // forward samples per list per iteration
   uint32_t per_row;         // proposals kept per join row
   uint64_t seed;
+  uint32_t learn_steps;     // training steps of the screen (0: default)
+  uint32_t learn_flags;     // TAGORE_LEARN_*
 };
+// Outcome of the learned screen in the last build on this thread.
+struct ScreenStats {
+  uint32_t used, steps, screened_iters, per_row, fallback;
+  float loss_first, loss_last;
+  double last_miss;       // improving pairs the screen did not keep (sampled nodes)
+  double last_best_kept;  // share of each row's exact best T the screen kept
+};
+void set_screen_stats(const ScreenStats& s);
 struct KnnStats {
   double ms_total, ms_prep, ms_iters;
   uint64_t proposals, pairs;

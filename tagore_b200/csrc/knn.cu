@@ -26,6 +26,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include "knn_shared.cuh"
+#include "mlp.cuh"
 
 namespace tagore {
 namespace knn {
@@ -179,7 +180,10 @@ __global__ void __launch_bounds__(128)
 // Plain local join: every pair with a new endpoint computed once with FP32
 // SIMT arithmetic (thread per pair, reference lane order), kept in a shared
 // distance matrix; each row then proposes its `per_row` closest partners.
-template <int D>
+// kStaged: the join-list rows are copied into shared memory first (rows up
+// to about 300 dims); otherwise each pair reads its two rows from the cache
+// hierarchy.
+template <int D, bool kStaged>
 __global__ void __launch_bounds__(128)
     k_join_plain(const uint64_t* __restrict__ nb, const __half* __restrict__ data, uint32_t n,
                  uint32_t dim_rt, uint32_t K, uint32_t T, uint32_t P,
@@ -204,14 +208,18 @@ __global__ void __launch_bounds__(128)
       kth[tid] = kth_of(nb[(size_t)list[tid] * K + K - 1]);
     }
     __syncthreads();
-    for (uint32_t r = warp; r < total; r += 4) {
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(data + (size_t)list[r] * dim);
-      for (uint32_t w = lane; w < dim / 2; w += 32) vec[r * words + w] = __ldg(src + w);
+    if (kStaged) {
+      for (uint32_t r = warp; r < total; r += 4) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(data + (size_t)list[r] * dim);
+        for (uint32_t w = lane; w < dim / 2; w += 32) vec[r * words + w] = __ldg(src + w);
+      }
     }
     __syncthreads();
     for (uint32_t r = 0; r < nn; ++r) {
       for (uint32_t c = r + 1 + tid; c < total; c += blockDim.x) {
-        const float d = thread_dist<D>(vec + r * words, vec + c * words, dim);
+        const float d = kStaged ? thread_dist<D>(vec + r * words, vec + c * words, dim)
+                                : row_dist(data + (size_t)list[r] * dim,
+                                           data + (size_t)list[c] * dim, dim);
         dm[r * (kMaxList + 1) + c] = d;
         dm[c * (kMaxList + 1) + r] = d;
         ++pairs;
@@ -316,14 +324,192 @@ int sm_count() {
 template <int D>
 int launch_join_plain(const Work& w, cudaStream_t s) {
   const uint32_t words = w.dim / 2 + 1;
-  const size_t sm = (size_t)2 * kMaxList * 4 + (size_t)kMaxList * (kMaxList + 1) * 4 +
-                    (size_t)kMaxList * words * 4;
-  if (sm > 227 * 1024) return fail(TAGORE_EINVAL, "plain join: DIM %u too large", w.dim);
-  TG_CUDA(cudaFuncSetAttribute((const void*)k_join_plain<D>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  const size_t base = (size_t)2 * kMaxList * 4 + (size_t)kMaxList * (kMaxList + 1) * 4;
+  const size_t staged = base + (size_t)kMaxList * words * 4;
+  const bool stage = staged <= 227 * 1024;
+  const size_t sm = stage ? staged : base;
+  const void* fn = stage ? (const void*)k_join_plain<D, true> : (const void*)k_join_plain<D, false>;
+  TG_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   const int grid = sm_count() * std::max(1, (int)((227 * 1024) / (sm + 1024)));
-  k_join_plain<D><<<grid, 128, sm, s>>>(w.nb, w.data, w.n, w.dim, w.K, w.T, w.P, w.lists, w.lcnt,
-                                        w.pool, w.stats);
+  if (stage)
+    k_join_plain<D, true><<<grid, 128, sm, s>>>(w.nb, w.data, w.n, w.dim, w.K, w.T, w.P, w.lists,
+                                                w.lcnt, w.pool, w.stats);
+  else
+    k_join_plain<D, false><<<grid, 128, sm, s>>>(w.nb, w.data, w.n, w.dim, w.K, w.T, w.P, w.lists,
+                                                 w.lcnt, w.pool, w.stats);
+  TG_CUDA(cudaGetLastError());
+  return TAGORE_OK;
+}
+
+// Local join screened by the learned projection z (n x 32, FP16). Each row
+// keeps its T candidates closest in projected distance; the kept pairs are
+// pooled per node and re-ranked with the exact reference-order FP32 distance
+// of the two base rows, and a pair is proposed only when that beats the row's
+// k-th entry. On every `sample_every`-th node the block also scores every
+// pair exactly and counts the improving pairs (exact distance below the row's
+// k-th) and how many of them the screen kept, stats[5] and stats[6], and
+// the rows' exact best T candidates and how many the screen kept, stats[8]
+// and stats[9].
+constexpr uint32_t kLearnedMaxT = 8;
+__global__ void __launch_bounds__(128)
+    k_join_learned(const uint64_t* __restrict__ nb, const __half* __restrict__ data,
+                   const __half* __restrict__ z, uint32_t n, uint32_t dim, uint32_t K, uint32_t T,
+                   uint32_t P, const uint32_t* __restrict__ lists, const uint32_t* __restrict__ lcnt,
+                   unsigned long long* __restrict__ pool, unsigned long long* __restrict__ stats,
+                   uint32_t sample_every) {
+  __shared__ float zs[kMaxList][mlp::kOut + 1];
+  __shared__ uint32_t ids[kMaxList];
+  __shared__ float kth[kMaxList];
+  __shared__ uint32_t pairs[kMaxList * kLearnedMaxT];
+  __shared__ uint32_t warp_cnt[4];
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  unsigned long long props = 0, exact = 0, rows = 0, improving = 0, found = 0, best = 0,
+                     best_kept = 0;
+  for (uint32_t u = blockIdx.x; u < n; u += gridDim.x) {
+    const uint32_t nn = lcnt[2 * u], total = lcnt[2 * u + 1];
+    if (nn == 0 || total < 2) continue;
+    if (tid == 0) rows += total;
+    const uint32_t r = tid;
+    const bool live = r < total;
+    if (live) {
+      const uint32_t id = lists[(size_t)u * kMaxList + r];
+      ids[r] = id;
+      kth[r] = kth_of(nb[(size_t)id * K + K - 1]);
+      const uint4* src = reinterpret_cast<const uint4*>(z + (size_t)id * mlp::kOut);
+#pragma unroll
+      for (int q = 0; q < mlp::kOut / 8; ++q) {
+        const uint4 v = __ldg(src + q);
+        const __half2* h = reinterpret_cast<const __half2*>(&v);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const float2 f = __half22float2(h[e]);
+          zs[r][q * 8 + 2 * e] = f.x;
+          zs[r][q * 8 + 2 * e + 1] = f.y;
+        }
+      }
+    }
+    __syncthreads();
+    // screen: the row's T closest columns in projected distance
+    const uint32_t cmax = live ? ((r < nn) ? total : nn) : 0u;
+    float zr[mlp::kOut];
+#pragma unroll
+    for (int o = 0; o < mlp::kOut; ++o) zr[o] = live ? zs[r][o] : 0.0f;
+    float bd[kLearnedMaxT];
+    uint32_t bc[kLearnedMaxT];
+#pragma unroll
+    for (int t = 0; t < (int)kLearnedMaxT; ++t) {
+      bd[t] = (uint32_t)t < T ? INFINITY : -INFINITY;
+      bc[t] = kInv;
+    }
+    for (uint32_t c = 0; c < total; ++c) {
+      float pd = 0.0f;
+#pragma unroll
+      for (int o = 0; o < mlp::kOut; ++o) {
+        const float e = zr[o] - zs[c][o];
+        pd = fmaf(e, e, pd);
+      }
+      float worst = bd[0];
+#pragma unroll
+      for (int t = 1; t < (int)kLearnedMaxT; ++t) worst = (uint32_t)t < T ? bd[t] : worst;
+      if (c < cmax && c != r && pd < worst) {
+        float v = pd;
+        uint32_t vc = c;
+#pragma unroll
+        for (int t = 0; t < (int)kLearnedMaxT; ++t)
+          if (v < bd[t]) {
+            swap_(v, bd[t]);
+            swap_(vc, bc[t]);
+          }
+      }
+    }
+    // pooled exact re-rank of the kept pairs
+    uint32_t kept = 0;
+#pragma unroll
+    for (int t = 0; t < (int)kLearnedMaxT; ++t) kept += bc[t] != kInv ? 1u : 0u;
+    uint32_t incl = kept;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, incl, o);
+      if (lane >= (uint32_t)o) incl += v;
+    }
+    if (lane == 31) warp_cnt[warp] = incl;
+    __syncthreads();
+    uint32_t off = incl - kept, npairs = 0;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      if ((uint32_t)w < warp) off += warp_cnt[w];
+      npairs += warp_cnt[w];
+    }
+#pragma unroll
+    for (int t = 0; t < (int)kLearnedMaxT; ++t)
+      if (bc[t] != kInv) pairs[off++] = (r << 16) | bc[t];
+    __syncthreads();
+    for (uint32_t q = tid; q < npairs; q += blockDim.x) {
+      const uint32_t pr = pairs[q], row = pr >> 16, col = pr & 0xFFFFu;
+      const float d = row_dist(data + (size_t)ids[row] * dim, data + (size_t)ids[col] * dim, dim);
+      ++exact;
+      if (d < kth[row]) {
+        propose(pool, ids[row], P, ids[col], d);
+        ++props;
+      }
+    }
+    // measurement on a sample of nodes: every pair exactly. Improving pairs
+    // (exact distance below the row's k-th) and how many the screen kept steer
+    // T; the row's exact best T and how many of them the screen kept measure
+    // how well the projection ranks.
+    if (sample_every && u % sample_every == 0 && live) {
+      float ed[kLearnedMaxT];
+      uint32_t ec[kLearnedMaxT];
+#pragma unroll
+      for (int t = 0; t < (int)kLearnedMaxT; ++t) {
+        ed[t] = (uint32_t)t < T ? INFINITY : -INFINITY;
+        ec[t] = kInv;
+      }
+      for (uint32_t c = 0; c < cmax; ++c) {
+        if (c == r) continue;
+        const float d = row_dist(data + (size_t)ids[r] * dim, data + (size_t)ids[c] * dim, dim);
+        bool kept_c = false;
+#pragma unroll
+        for (int t = 0; t < (int)kLearnedMaxT; ++t) kept_c |= bc[t] == c;
+        if (d < kth[r]) {
+          ++improving;
+          found += kept_c ? 1u : 0u;
+        }
+        float v = d;
+        uint32_t vc = c;
+#pragma unroll
+        for (int t = 0; t < (int)kLearnedMaxT; ++t)
+          if (v < ed[t]) {
+            swap_(v, ed[t]);
+            swap_(vc, ec[t]);
+          }
+      }
+#pragma unroll
+      for (int t = 0; t < (int)kLearnedMaxT; ++t) {
+        if (ec[t] == kInv) continue;
+        ++best;
+        bool kept_c = false;
+#pragma unroll
+        for (int q = 0; q < (int)kLearnedMaxT; ++q) kept_c |= bc[q] == ec[t];
+        best_kept += kept_c ? 1u : 0u;
+      }
+    }
+    __syncthreads();
+  }
+  if (props) atomicAdd(&stats[0], props);
+  if (exact) atomicAdd(&stats[1], exact);
+  if (tid == 0 && rows) atomicAdd(&stats[3], rows);
+  if (improving) atomicAdd(&stats[5], improving);
+  if (found) atomicAdd(&stats[6], found);
+  if (best) atomicAdd(&stats[8], best);
+  if (best_kept) atomicAdd(&stats[9], best_kept);
+}
+
+int join_learned(const Work& w, const __half* z, uint32_t T, uint32_t sample_every,
+                 cudaStream_t s) {
+  const int grid = sm_count() * 8;
+  k_join_learned<<<grid, 128, 0, s>>>(w.nb, w.data, z, w.n, w.dim, w.K, T, w.P, w.lists, w.lcnt,
+                                      w.pool, w.stats, sample_every);
   TG_CUDA(cudaGetLastError());
   return TAGORE_OK;
 }
@@ -344,6 +530,7 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   if (a.k > 128) return fail(TAGORE_EINVAL, "K must be <= 128 (got %u)", a.k);
   if (d.dim % 4) return fail(TAGORE_EINVAL, "DIM must be a multiple of 4 (got %u)", d.dim);
   if (d.n >= 0x7FFFFFFFu) return fail(TAGORE_EINVAL, "POINTS must be < 2^31");
+  if (a.mode > TAGORE_KNN_LEARNED) return fail(TAGORE_EINVAL, "unknown kNN mode %u", a.mode);
   const uint32_t S = std::min<uint32_t>(a.sample ? a.sample : 32, kMaxS);
   const uint32_t T = std::min<uint32_t>(a.per_row ? a.per_row : 2,
                                         a.mode == TAGORE_KNN_PLAIN ? kMaxT : 4u);
@@ -361,7 +548,7 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   const size_t nbB = (size_t)d.n * K * 8, poolB = (size_t)d.n * P * 8;
   const size_t listB = (size_t)d.n * S * 4;
   Scratch sc(s);
-  TG_TRY(sc.alloc(nbB + poolB + 4 * listB + (size_t)d.n * kMaxList * 4 + (size_t)d.n * 24 + 128));
+  TG_TRY(sc.alloc(nbB + poolB + 4 * listB + (size_t)d.n * kMaxList * 4 + (size_t)d.n * 24 + 256));
   unsigned char* p = sc.as<unsigned char>();
   w.nb = reinterpret_cast<uint64_t*>(p);
   p += nbB;
@@ -378,7 +565,7 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   w.stats = reinterpret_cast<unsigned long long*>(
       (reinterpret_cast<uintptr_t>(w.lcnt + (size_t)d.n * 2) + 15) & ~(uintptr_t)15);
   TG_CUDA(cudaMemsetAsync(w.pool, 0xFF, poolB, s));
-  TG_CUDA(cudaMemsetAsync(w.stats, 0, 64, s));
+  TG_CUDA(cudaMemsetAsync(w.stats, 0, 128, s));
   const int sms = sm_count();
   const uint64_t n64 = d.n;
   stage_begin("knn_init", s);
@@ -387,6 +574,18 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   stage_end("knn_init", s, n64 * K * (2ull * d.dim + 8), n64 * K);
   TG_CUDA(cudaGetLastError());
   const char* join_name = a.mode == TAGORE_KNN_PLAIN ? "knn_join_plain" : "knn_join_tc";
+  // The learned screen serves the chosen path where the tensor-core tile does
+  // not apply (and every width when asked for): the first iterations run the
+  // exact join, then the MLP is trained on their rows and screens the rest.
+  const bool learned = a.mode == TAGORE_KNN_LEARNED ||
+                       (a.mode == TAGORE_KNN_CHOSEN && !tc_supported(d.dim));
+  const uint32_t warm = std::min<uint32_t>(2, a.iters);
+  uint32_t lt = a.per_row ? std::min<uint32_t>(std::max<uint32_t>(a.per_row, 2), kLearnedMaxT) : 4;
+  const bool adapt = !(a.learn_flags & TAGORE_LEARN_FIXED_T);
+  bool fallback = false;
+  mlp::Net net;
+  Scratch zbuf(s);
+  ScreenStats sst{};
   for (uint32_t it = 0; it < a.iters; ++it) {
     TG_CUDA(cudaMemsetAsync(w.rcnt, 0, (size_t)d.n * 8, s));
     stage_begin("knn_sample", s);
@@ -401,14 +600,55 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
     count_launch();
     stage_end("knn_lists", s, n64 * 4 * S * 4 + n64 * kMaxList * 4, n64);
     TG_CUDA(cudaGetLastError());
-    stage_begin(join_name, s);
-    if (a.mode == TAGORE_KNN_PLAIN) {
-      TG_TRY(join_plain(w, s));
-    } else {
-      TG_TRY(join_tc(w, s));
+    if (learned && it == warm && !fallback) {
+      stage_begin("mlp_train", s);
+      TG_TRY(net.init(d.dim, a.seed ^ 0x5C4EE17ull, s));
+      TG_TRY(net.center(d.data, d.n, s));
+      const uint32_t steps = (a.learn_flags & TAGORE_LEARN_NO_TRAIN)
+                                 ? 0u
+                                 : (a.learn_steps ? a.learn_steps : 400u);
+      if (steps) {
+        TG_TRY(net.train(w.nb, d.n, K, d.data, steps, 4096, a.seed + it, &sst.loss_first,
+                         &sst.loss_last, s));
+      }
+      sst.steps = steps;
+      stage_end("mlp_train", s, (uint64_t)steps * 3 * 4096 * (2ull * d.dim), (uint64_t)steps * 4096);
+      stage_begin("mlp_project", s);
+      TG_TRY(zbuf.alloc((size_t)d.n * mlp::kOut * 2));
+      TG_TRY(net.project(d.data, d.n, zbuf.as<__half>(), s));
+      stage_end("mlp_project", s, n64 * (2ull * d.dim + 2ull * mlp::kOut), n64);
     }
-    count_launch();
-    stage_end(join_name, s);
+    if (learned && it >= warm && !fallback) {
+      stage_begin("knn_join_learned", s);
+      TG_CUDA(cudaMemsetAsync(w.stats + 5, 0, 5 * 8, s));
+      TG_TRY(join_learned(w, zbuf.as<__half>(), lt, 256, s));
+      count_launch();
+      stage_end("knn_join_learned", s);
+      unsigned long long h2[5] = {0, 0, 0, 0, 0};
+      TG_CUDA(cudaMemcpyAsync(h2, w.stats + 5, sizeof(h2), cudaMemcpyDeviceToHost, s));
+      TG_CUDA(cudaStreamSynchronize(s));
+      sst.last_best_kept = h2[3] ? (double)h2[4] / (double)h2[3] : 0.0;
+      // miss rate of the screen on the sampled nodes steers the kept count;
+      // a screen that misses most improving pairs even at the largest count
+      // hands the remaining iterations to the exact join
+      const double miss = h2[0] ? 1.0 - (double)h2[1] / (double)h2[0] : 0.0;
+      sst.last_miss = miss;
+      sst.screened_iters += 1;
+      if (adapt) {
+        if (miss > 0.10 && lt < kLearnedMaxT) lt = std::min<uint32_t>(kLearnedMaxT, lt + 2);
+        else if (miss < 0.02 && lt > 2) lt -= 1;
+        if (miss > 0.5 && lt == kLearnedMaxT) fallback = true;
+      }
+    } else {
+      stage_begin(join_name, s);
+      if (a.mode == TAGORE_KNN_PLAIN || !tc_supported(w.dim)) {
+        TG_TRY(join_plain(w, s));
+      } else {
+        TG_TRY(join_tc(w, s));
+      }
+      count_launch();
+      stage_end(join_name, s);
+    }
     stage_begin("knn_merge", s);
     k_merge<<<sms * 16, 128, 0, s>>>(w.nb, w.pool, d.n, K, P, w.stats);
     count_launch();
@@ -429,6 +669,10 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
     st->proposals = h[0];
     st->pairs = h[1];
   }
+  sst.used = learned ? 1u : 0u;
+  sst.per_row = lt;
+  sst.fallback = fallback ? 1u : 0u;
+  set_screen_stats(sst);
   return TAGORE_OK;
 }
 

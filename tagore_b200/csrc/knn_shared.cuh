@@ -22,10 +22,14 @@ struct Work {
   uint32_t *fnew, *fold, *rnew, *rold, *fcnt, *rcnt;
   uint32_t* lists;  // [n][128] join lists: new ids first, then old
   uint32_t* lcnt;   // [n][2] (new count, total)
-  unsigned long long* stats;  // [0] proposals, [1] exact pairs, [2] row updates, [4] error flag
+  // [0] proposals, [1] exact pairs, [2] row updates, [3] rows gathered, [4] error flag,
+  // [5..9] learned-screen measurements (16 slots)
+  unsigned long long* stats;
 };
 
 int join_tc(const Work& w, cudaStream_t s);
+// Row widths the tensor-core join takes (one 128-row tile of K-major FP16).
+inline bool tc_supported(uint32_t dim) { return dim >= 16 && dim <= 128 && dim % 16 == 0; }
 
 __device__ __forceinline__ uint64_t make_key(float d, uint32_t id, bool is_new) {
   return ((uint64_t)__float_as_uint(d) << 32) | ((uint64_t)id << 1) | (is_new ? 1ull : 0ull);

@@ -47,3 +47,21 @@ def test_knn_recall(capi, orc, mode):
     truth, _ = orc.exact_knn(half, K)
     r = recall_at(g, truth, 10)
     assert r > 0.95, r
+
+
+@pytest.mark.parametrize("kind,dim", [("deep", 96), ("gist", 960), ("sift", 200)])
+@pytest.mark.parametrize("mode", ["plain", "chosen"])
+def test_knn_other_widths(capi, orc, kind, dim, mode):
+    """Row widths beside 128: 96 (tensor-core screen), 960 and 200 (rows read
+    from the cache hierarchy; the chosen mode falls back to the plain join)."""
+    base, _ = synth.mixture(kind, 4000, dim, 16, 23)
+    K = 32
+    g, d, half = build(capi, base, K, 8, capi.KNN_PLAIN if mode == "plain" else capi.KNN_CHOSEN)
+    n = base.shape[0]
+    assert (g < n).all()
+    assert not (g == np.arange(n)[:, None]).any()
+    assert (np.diff(d, axis=1) >= 0).all()
+    exp = orc.dist_pairs(half, np.repeat(np.arange(n), K), g.reshape(-1)).reshape(n, K)
+    assert np.array_equal(d.view(np.uint32), exp.view(np.uint32))
+    truth, _ = orc.exact_knn(half, K)
+    assert recall_at(g, truth, 10) > 0.9
