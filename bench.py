@@ -275,6 +275,12 @@ def main():
             ep = capi.pruning_cfs(st, FD, "path", "dist", topm=TOPM, thre=THRE)
             rows = st.download(0).reshape(n, K)
             extra[f"index_recall10_{label}"] = index_recall(rows, ep, base, queries, half_t)
+            if label == "chosen":
+                # the opt-in connectivity fix (edges appended; not part of the timed build)
+                extra["connect_edges_added"] = capi.connect(st, ep)
+                rows = st.download(0).reshape(n, K)
+                extra["index_recall10_chosen_connected"] = index_recall(rows, ep, base, queries,
+                                                                        half_t)
             st.free()
 
     e2e = None

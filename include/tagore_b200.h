@@ -139,6 +139,15 @@ int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int 
 int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_rows,
                        const uint32_t* local_medoids);
 
+/* No counterpart in the reference (opt-in; it changes the edge lists): makes
+ * every node of the pruned graph in st->graph ([deg, ids...] rows, stride K)
+ * reachable from `ep` by appending edges, in the manner of NSG's tree
+ * growing. An unreachable node is attached to the end of a greedy walk from
+ * ep toward it. *added receives the number of edges added. Call it after
+ * tagore_pruning / tagore_pruning_cfs and before writing an index from the
+ * rows. */
+int tagore_connect(TagoreKnnState* st, uint32_t ep, uint64_t* added);
+
 /* cal_ep_gpu (src/Tagore_src.cu:1889-2058) alone: entry point of the graph
  * held in st (kNN rows) toward st->center. */
 int tagore_entry_point(TagoreKnnState* st, uint32_t topm, uint32_t* ep);

@@ -84,6 +84,7 @@ SIGNATURES = {
     "tagore_large_index": (C.c_int, [C.POINTER(LargeParams), C.c_void_p, C.c_int]),
     "tagore_large_merge": (C.c_int, [C.POINTER(LargeParams), C.POINTER(C.c_void_p), C.c_void_p]),
     "tagore_entry_point": (C.c_int, [C.POINTER(KnnState), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "tagore_connect": (C.c_int, [C.POINTER(KnnState), C.c_uint32, C.POINTER(C.c_uint64)]),
     "tagore_state_alloc": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KnnState)]),
     "tagore_state_free": (C.c_int, [C.POINTER(KnnState)]),
     "tagore_state_upload": (C.c_int, [C.POINTER(KnnState), C.c_int, C.c_void_p, C.c_size_t]),
@@ -244,6 +245,13 @@ def pruning_cfs_noalloc(state, final_degree, mode, metric, topm=64, thre=1.0, st
     check(lib().tagore_pruning_cfs_noalloc(C.byref(p), C.byref(st), mode.encode(), metric.encode(),
                                            stream))
     return st.ep
+
+
+def connect(state, ep):
+    """Opt-in connectivity fix; returns the number of edges added."""
+    added = C.c_uint64(0)
+    check(lib().tagore_connect(C.byref(state.st), ep, C.byref(added)))
+    return added.value
 
 
 def entry_point(state, topm=64):

@@ -479,6 +479,13 @@ int tagore_gnn_descent(const TagoreKnnParams* p, const char* fvecs_path, TagoreK
   return tagore_gnn_descent_host(p, host.data(), n, dim, out);
 }
 
+int tagore_connect(TagoreKnnState* st, uint32_t ep, uint64_t* added) {
+  TG_TRY(check_state(st));
+  Stream s;
+  TG_TRY(s.init());
+  return connect_graph(dev_of(st), ep, added, s.s);
+}
+
 int tagore_entry_point(TagoreKnnState* st, uint32_t topm, uint32_t* ep) {
   TG_TRY(check_state(st));
   if (!ep || topm == 0) return fail(TAGORE_EINVAL, "bad entry-point arguments");

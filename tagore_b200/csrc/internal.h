@@ -97,6 +97,9 @@ int prune_cfs(const Dev& d, const PruneArgs& a, const std::string& mode, const s
               uint32_t* ep_host, cudaStream_t s);
 // Individual stages, exposed for the stage-level parity tests.
 int stage_cal_ep(const Dev& d, uint32_t topm, uint32_t* ep_host, cudaStream_t s);
+// Opt-in connectivity fix of pruned rows ([deg, ids] stride K): edges are
+// appended until every node is reachable from ep (connect.cu).
+int connect_graph(const Dev& d, uint32_t ep, uint64_t* added, cudaStream_t s);
 // Size of the per-device static scratch of prune_cfs_static.
 constexpr size_t kStaticScratchBytes = (size_t)16 << 20;
 // prune_cfs for path|2-hop with dist|angle with every temporary carved from
