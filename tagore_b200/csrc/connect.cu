@@ -12,7 +12,7 @@
 //      walks greedily from ep toward u (exact reference-order distances; all
 //      walks finish before any row changes), then u is appended to the row of
 //      the walk's end node v, which is reachable; when v's row is full the
-//      walk's previous nodes are tried;
+//      walk's previous nodes, then hashed reachable nodes, are tried;
 //   3. BFS again from the attached nodes; repeat until all are reachable.
 #include "common.cuh"
 #include "internal.h"
@@ -20,8 +20,10 @@
 namespace tagore {
 namespace {
 
-constexpr uint32_t kBatch = 4096;  // unreachable nodes attached per round
-constexpr uint32_t kWalk = 256;    // greedy steps per walk
+constexpr uint32_t kBatch = 256;  // unreachable nodes attached per round
+constexpr uint32_t kWalk = 256;   // greedy steps per walk
+constexpr int kEnds = 8;          // walk nodes kept as attach points, end first
+constexpr int kProbe = 64;        // hashed reachable nodes tried after them
 
 // One BFS level: every frontier node marks its unmarked out-neighbours and
 // appends them to the next frontier. Warp per frontier node.
@@ -78,7 +80,7 @@ __global__ void k_unreached(const uint32_t* __restrict__ reach, uint32_t n, uint
 }
 
 // For each listed node u: a greedy walk from ep toward u over the rows (the
-// closest out-neighbour while it is closer), recording the walk's last four
+// closest out-neighbour while it is closer), recording the walk's last kEnds
 // nodes, end first. All of them are reachable from ep. Reads rows only.
 __global__ void k_walk(const uint32_t* __restrict__ rows, uint32_t K, uint32_t n,
                        const __half* __restrict__ data, uint32_t dim, uint32_t ep,
@@ -89,7 +91,9 @@ __global__ void k_walk(const uint32_t* __restrict__ rows, uint32_t K, uint32_t n
        t += (gridDim.x * blockDim.x) >> 5) {
     const uint32_t u = todo[t];
     const __half* q = data + (size_t)u * dim;
-    uint32_t path[4] = {ep, ep, ep, ep};
+    uint32_t path[kEnds];
+#pragma unroll
+    for (int h = 0; h < kEnds; ++h) path[h] = ep;
     uint32_t cur = ep;
     float cd = warp_dist(q, data + (size_t)ep * dim, dim, lane);
     for (uint32_t step = 0; step < kWalk; ++step) {
@@ -121,38 +125,53 @@ __global__ void k_walk(const uint32_t* __restrict__ rows, uint32_t K, uint32_t n
         }
       }
       if (bid == cur) break;  // local minimum
-      path[3] = path[2];
-      path[2] = path[1];
-      path[1] = path[0];
+#pragma unroll
+      for (int h = kEnds - 1; h > 0; --h) path[h] = path[h - 1];
       path[0] = bid;
       cur = bid;
       cd = best;
     }
-    if (lane < 4) ends[(size_t)t * 4 + lane] = path[lane];
+#pragma unroll
+    for (int h = 0; h < kEnds; ++h)
+      if (lane == (uint32_t)h) ends[(size_t)t * kEnds + h] = path[h];
   }
 }
 
 // Appends each listed node u to the first row among its walk's ends that has
-// a free slot; attached nodes start the next BFS.
-__global__ void k_append(uint32_t* __restrict__ rows, uint32_t K, const uint32_t* __restrict__ todo,
-                         uint32_t ntodo, const uint32_t* __restrict__ ends,
-                         uint32_t* __restrict__ reach, uint32_t* __restrict__ front,
-                         uint32_t* __restrict__ nfront, unsigned long long* __restrict__ added) {
+// a free slot; when all of them are full (walks that cannot leave the
+// reachable part all end at the same few nodes), to a reachable node with a
+// free slot found by hashed probing. Attached nodes start the next BFS.
+__global__ void k_append(uint32_t* __restrict__ rows, uint32_t K, uint32_t n,
+                         const uint32_t* __restrict__ todo, uint32_t ntodo,
+                         const uint32_t* __restrict__ ends, uint32_t* __restrict__ reach,
+                         uint32_t* __restrict__ front, uint32_t* __restrict__ nfront,
+                         unsigned long long* __restrict__ added) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntodo) return;
   const uint32_t u = todo[t];
-  for (int h = 0; h < 4; ++h) {
-    const uint32_t v = ends[(size_t)t * 4 + h];
-    if (v == u) continue;
+  auto try_row = [&](uint32_t v) -> bool {
+    if (v == u || v >= n) return false;
     uint32_t* row = rows + (size_t)v * K;
     const uint32_t slot = atomicAdd(&row[0], 1u);
     if (slot + 1 < K) {
       row[1 + slot] = u;
-      atomicAdd(added, 1ull);
-      if (atomicExch(&reach[u], 1u) == 0u) front[atomicAdd(nfront, 1u)] = u;
-      return;
+      return true;
     }
     atomicSub(&row[0], 1u);
+    return false;
+  };
+  bool done = false;
+  for (int h = 0; h < kEnds && !done; ++h) done = try_row(ends[(size_t)t * kEnds + h]);
+  uint64_t x = 0x9E3779B97F4A7C15ull * (uint64_t)(u + 1);
+  for (int p = 0; p < kProbe && !done; ++p) {
+    x ^= x >> 29;
+    x *= 0xBF58476D1CE4E5B9ull;
+    const uint32_t v = (uint32_t)(x % n);
+    if (reach[v] == 1u && v != u) done = try_row(v);
+  }
+  if (done) {
+    atomicAdd(added, 1ull);
+    if (atomicExch(&reach[u], 1u) == 0u) front[atomicAdd(nfront, 1u)] = u;
   }
 }
 
@@ -163,13 +182,13 @@ int connect_graph(const Dev& d, uint32_t ep, uint64_t* added_out, cudaStream_t s
   if (d.k < 2) return fail(TAGORE_EINVAL, "K must be >= 2");
   Scratch sc(s);
   const size_t n = d.n;
-  TG_TRY(sc.alloc(16 + n * 4 * 3 + (size_t)kBatch * 16));
+  TG_TRY(sc.alloc(16 + n * 4 * 3 + (size_t)kBatch * kEnds * 4));
   unsigned long long* added = sc.as<unsigned long long>();
   uint32_t* ctr = reinterpret_cast<uint32_t*>(added + 1);  // [0] frontier size, [1] unreachable
   uint32_t* reach = ctr + 2;
   uint32_t* fa = reach + n;
   uint32_t* fb = fa + n;
-  uint32_t* ends = fb + n;  // [kBatch][4] walk ends
+  uint32_t* ends = fb + n;  // [kBatch][kEnds] walk ends
   TG_CUDA(cudaMemsetAsync(added, 0, 16 + n * 4, s));  // counters and reach
   const uint32_t one = 1;
   TG_CUDA(cudaMemcpyAsync(reach + ep, &one, 4, cudaMemcpyHostToDevice, s));
@@ -210,8 +229,8 @@ int connect_graph(const Dev& d, uint32_t ep, uint64_t* added_out, cudaStream_t s
     // the nodes to attach are listed in fb; attached nodes start the next BFS in fa
     k_walk<<<std::min<uint32_t>((todo + 7) / 8, (uint32_t)sms * 16), 256, 0, s>>>(
         d.graph, d.k, d.n, d.data, d.dim, ep, fb, todo, ends);
-    k_append<<<(todo + 255) / 256, 256, 0, s>>>(d.graph, d.k, fb, todo, ends, reach, fa, ctr,
-                                                added);
+    k_append<<<(todo + 255) / 256, 256, 0, s>>>(d.graph, d.k, d.n, fb, todo, ends, reach, fa,
+                                                ctr, added);
     count_launch(2);
     TG_CUDA(cudaGetLastError());
     TG_CUDA(cudaMemcpyAsync(&nfront, ctr, 4, cudaMemcpyDeviceToHost, s));
