@@ -115,7 +115,7 @@ int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const cha
 /* No counterpart in the reference. Same result as tagore_pruning_cfs for
  * mode 'path' or '2-hop' with metric 'dist' or 'angle', computed without
  * allocating device memory: every temporary comes from one static device
- * array of 16 MiB per device (about 20,000 points at FINAL_DEGREE 32).
+ * array of 16 MiB per device (about 18,000 points at FINAL_DEGREE 32).
  * Graphs whose temporaries do not fit, and other mode/metric pairs, return
  * TAGORE_EINVAL. Work goes to `stream` (a cudaStream_t; NULL is the legacy
  * default stream) and the call returns after it has finished. Calls that

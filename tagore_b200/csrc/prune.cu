@@ -497,11 +497,15 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
   return nsel;
 }
 
-// Per-warp shared layout of the select kernels.
+// Per-warp shared layout of the select kernels: the beam (path collect) and
+// the candidate list share one region, since the list is filled only after
+// the beam has finished (its ring of scored nodes lives in global memory).
 struct SelLayout {
   uint32_t W, L, fd;
   __host__ __device__ size_t bytes() const {
-    return (W ? beam_bytes(W) : 0) + (size_t)L * 8 + (size_t)fd * 8 + 64;
+    const size_t list = (size_t)L * 8 + (size_t)fd * 8;
+    const size_t beam = W ? beam_bytes(W) : 0;
+    return ((beam > list ? beam : list) + 64 + 15) & ~(size_t)15;
   }
 };
 
@@ -538,13 +542,16 @@ __device__ __forceinline__ uint32_t next_node(uint32_t* ctr, int lane) {
   return __shfl_sync(kFull, b, 0);
 }
 
+// ring_ids / ring_dis: per-warp rings of kSelectCand scored nodes (path
+// collect), indexed by the warp's global number.
 template <bool kPath>
 __global__ void __launch_bounds__(kWarps * 32, 6)
     k_select(const uint32_t* __restrict__ G, float* __restrict__ nd, const __half* __restrict__ data,
              uint32_t n, uint32_t dim, uint32_t K, const uint32_t* __restrict__ ep_dev,
              uint32_t* __restrict__ ctr, uint32_t topm, uint32_t fd, float thre,
              uint32_t* __restrict__ P_ids, float* __restrict__ P_dis, uint32_t* __restrict__ P_cnt,
-             unsigned long long* __restrict__ work) {
+             unsigned long long* __restrict__ work, uint32_t* __restrict__ ring_ids,
+             float* __restrict__ ring_dis) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   SelLayout lay{kPath ? topm + K : 0u, kSelectCand + K, fd};
@@ -553,7 +560,10 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
   float* cdis = reinterpret_cast<float*>(cand + lay.L);
   uint32_t* sel = reinterpret_cast<uint32_t*>(cdis + lay.L);
   float* seld = reinterpret_cast<float*>(sel + fd);
-  Beam bm = beam_carve(reinterpret_cast<unsigned char*>(seld + fd), lay.W);
+  Beam bm = beam_carve(mine, lay.W);  // same region as the list, used before it
+  const size_t gw = (size_t)blockIdx.x * kWarps + warp;
+  uint32_t* rid = kPath ? ring_ids + gw * kSelectCand : nullptr;
+  float* rds = kPath ? ring_dis + gw * kSelectCand : nullptr;
   const uint32_t L = lay.L;
   const uint32_t ep = kPath ? *ep_dev : 0u;
   for (uint32_t b = next_node(ctr, lane); b < n; b = next_node(ctr, lane)) {
@@ -561,11 +571,13 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
     uint32_t scored = kSelectCand;  // rows scored for this node (2-hop: the 480 collected)
     if (kPath) {
       uint32_t curr = 0;
-      warp_beam(G, data, dim, K, q, ep, topm, 10, bm, cand + K, cdis + K, &curr, lane);
+      warp_beam(G, data, dim, K, q, ep, topm, 10, bm, rid, rds, &curr, lane);
       scored = curr;
-      for (uint32_t i = curr + lane; i < kSelectCand; i += 32) {
-        cand[K + i] = kInv;
-        cdis[K + i] = kInfDis;
+      __syncwarp();  // the ring (global) and the beam's region are done
+      for (uint32_t i = lane; i < kSelectCand; i += 32) {
+        const bool in = i < curr;
+        cand[K + i] = in ? rid[i] : kInv;
+        cdis[K + i] = in ? rds[i] : kInfDis;
       }
     } else {
       for (uint32_t i = lane; i < kSelectCand; i += 32) {
@@ -1054,6 +1066,11 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   TG_TRY(set_smem(fn, sm));
   int grid = 0;
   TG_TRY(resident_grid(fn, kWarps * 32, sm, kWarps, d.n, &grid));
+  Scratch rings(s);
+  if (path) TG_TRY(rings.alloc((size_t)grid * kWarps * kSelectCand * 8));
+  uint32_t* ring_ids = path ? rings.as<uint32_t>() : nullptr;
+  float* ring_dis =
+      path ? reinterpret_cast<float*>(ring_ids + (size_t)grid * kWarps * kSelectCand) : nullptr;
   uint32_t* ctr = ep_dev + 1;
   TG_CUDA(cudaMemsetAsync(work, 0, 8, s));
   TG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
@@ -1061,11 +1078,12 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   stage_begin(sel_name, s);
   if (path)
     k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev, ctr,
-                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt, work);
+                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt, work,
+                                                 ring_ids, ring_dis);
   else
     k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
                                                   ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt,
-                                                  work);
+                                                  work, nullptr, nullptr);
   count_launch();
   stage_end(sel_name, s);
   TG_CUDA(cudaGetLastError());
@@ -1208,7 +1226,19 @@ int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
   TG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_tmp, (uint32_t*)nullptr, (uint32_t*)nullptr,
                                         (int)d.n, s));
   const size_t tmp = std::max(sort_tmp, scan_tmp);
-  // Layout: flags | select rows | reverse-edge keys | CUB temporary.
+  // The select kernel's grid is capped here so that its per-warp rings of
+  // scored nodes (path collect) stay small: 64 blocks, under 1 MB.
+  SelLayout lay{path ? a.topm + K : 0u, kSelectCand + K, fd};
+  const size_t sm = lay.bytes() * kWarps;
+  const void* fn = path ? (const void*)k_select<true> : (const void*)k_select<false>;
+  TG_TRY(set_smem(fn, sm));
+  int grid = 0;
+  TG_TRY(resident_grid(fn, kWarps * 32, sm, kWarps, d.n, &grid));
+  grid = std::min(grid, 64);
+  const size_t ring_n = path ? (size_t)grid * kWarps * kSelectCand : 0;
+  // Layout: flags | select rows | reverse-edge keys | CUB temporary | rings.
+  uint32_t* ring_ids = nullptr;
+  float* ring_dis = nullptr;
   auto layout = [&](Carve& c, uint32_t** flags, uint32_t** P_ids, float** P_dis, uint32_t** P_cnt,
                     uint32_t** keys, uint32_t** vals, uint32_t** keys2, uint32_t** vals2,
                     uint32_t** deg, uint32_t** off, void** tmp_p) {
@@ -1223,6 +1253,8 @@ int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
     *deg = (uint32_t*)c.take((size_t)d.n * 4);
     *off = (uint32_t*)c.take((size_t)d.n * 4);
     *tmp_p = c.take(tmp);
+    ring_ids = (uint32_t*)c.take(ring_n * 4);
+    ring_dis = (float*)c.take(ring_n * 4);
   };
   uint32_t *flags, *P_ids, *P_cnt, *keys, *vals, *keys2, *vals2, *deg, *off;
   float* P_dis;
@@ -1260,19 +1292,14 @@ int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
     count_launch();
     TG_CUDA(cudaGetLastError());
   }
-  SelLayout lay{path ? a.topm + K : 0u, kSelectCand + K, fd};
-  const size_t sm = lay.bytes() * kWarps;
-  const void* fn = path ? (const void*)k_select<true> : (const void*)k_select<false>;
-  TG_TRY(set_smem(fn, sm));
-  int grid = 0;
-  TG_TRY(resident_grid(fn, kWarps * 32, sm, kWarps, d.n, &grid));
   if (path)
     k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev, ctr,
-                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt, nullptr);
+                                                 a.topm, fd, a.thre, P_ids, P_dis, P_cnt, nullptr,
+                                                 ring_ids, ring_dis);
   else
     k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
                                                   ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt,
-                                                  nullptr);
+                                                  nullptr, nullptr, nullptr);
   count_launch();
   TG_CUDA(cudaGetLastError());
 
