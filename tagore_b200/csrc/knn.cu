@@ -258,39 +258,103 @@ __global__ void __launch_bounds__(128)
   if (tid == 0) atomicAdd(&stats[3], rows);
 }
 
-// Merges the pool of each node into its sorted row and clears the pool.
+// Merges the pool of each node into its sorted row and clears the pool. Only
+// the pool entries closer than the row's k-th (m of them, usually few) are
+// sorted, in registers, and merged into the sorted row by rank; the merged
+// sequence is the one a full sort of row and pool would give (keys are
+// unique per pool slot, and a row key sorts before an equal pool key), and
+// repeats of (distance, id) keep their first copy as before.
+template <int E>
+__device__ __forceinline__ void sort_fresh(uint64_t* fb, uint32_t m, int lane) {
+  uint64_t k[E];
+#pragma unroll
+  for (int t = 0; t < E; ++t) {
+    const uint32_t j = lane + 32 * t;
+    k[t] = j < m ? fb[j] : kEmpty;
+  }
+  warp_sort_keys<E>(k, lane);
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < E; ++t) {
+    const uint32_t j = lane + 32 * t;
+    if (j < m) fb[j] = k[t];
+  }
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(128)
     k_merge(uint64_t* __restrict__ nb, unsigned long long* __restrict__ pool, uint32_t n,
             uint32_t K, uint32_t P, unsigned long long* __restrict__ stats) {
+  __shared__ uint64_t rows_s[4][kMaxList], fresh_s[4][kPool], merged_s[4][kMaxList + kPool];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  uint64_t* rb = rows_s[warp];
+  uint64_t* fb = fresh_s[warp];
+  uint64_t* mb = merged_s[warp];
   unsigned long long upd = 0;
   for (uint32_t u = blockIdx.x * 4 + warp; u < n; u += gridDim.x * 4) {
     uint64_t* row = nb + (size_t)u * K;
     unsigned long long* pl = pool + (size_t)u * P;
     const uint64_t kth = row[K - 1];
-    uint64_t keys[8];
-    // positions 0..127 hold the row (K <= 128), 128..255 the pool (P <= 128)
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const uint32_t j = lane + 32 * t;
-      keys[t] = (j < K) ? row[j] : kEmpty;
-    }
-    uint32_t fresh = 0;
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const uint32_t j = lane + 32 * t;
+    uint32_t m = 0;
+    for (uint32_t base = 0; base < P; base += 32) {
+      const uint32_t j = base + lane;
       uint64_t k = kEmpty;
       if (j < P) {
         k = pl[j];
         if (k != kEmpty) pl[j] = kEmpty;
-        if (!(k < kth)) k = kEmpty;
-        else ++fresh;
       }
-      keys[4 + t] = k;
+      const bool fresh = k < kth;
+      const unsigned mk = __ballot_sync(kFull, fresh);
+      if (fresh) fb[m + __popc(mk & lt)] = k;
+      m += __popc(mk);
     }
-    if (__reduce_add_sync(kFull, fresh) == 0) continue;
-    warp_sort_keys<8>(keys, lane);
-    upd += dedupe_store_row<8>(keys, lane, row, K);
+    if (m == 0) continue;
+    for (uint32_t j = lane; j < K; j += 32) rb[j] = row[j];
+    __syncwarp();
+    if (m <= 32) sort_fresh<1>(fb, m, lane);
+    else if (m <= 64) sort_fresh<2>(fb, m, lane);
+    else sort_fresh<4>(fb, m, lane);
+    // merged rank: row i -> i + #(fresh < r_i); fresh p -> p + #(row <= f_p)
+    for (uint32_t i = lane; i < K; i += 32) {
+      const uint64_t r = rb[i];
+      uint32_t lo = 0, hi = m;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (fb[mid] < r) lo = mid + 1;
+        else hi = mid;
+      }
+      mb[i + lo] = r;
+    }
+    for (uint32_t p = lane; p < m; p += 32) {
+      const uint64_t f = fb[p];
+      uint32_t lo = 0, hi = K;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (rb[mid] <= f) lo = mid + 1;
+        else hi = mid;
+      }
+      mb[p + lo] = f;
+    }
+    __syncwarp();
+    // first K distinct (distance, id) keys back to the row
+    const uint32_t total = K + m;
+    uint32_t out = 0, fresh_kept = 0;
+    for (uint32_t c = 0; c < total && out < K; c += 32) {
+      const uint32_t i = c + lane;
+      const uint64_t k = i < total ? mb[i] : kEmpty;
+      const bool keep = k != kEmpty && (i == 0 || (k >> 1) != (mb[i - 1] >> 1));
+      const unsigned mk = __ballot_sync(kFull, keep);
+      const uint32_t pos = out + __popc(mk & lt);
+      if (keep && pos < K) {
+        row[pos] = k;
+        fresh_kept += (uint32_t)(k & 1ull);
+      }
+      out += __popc(mk);
+    }
+    for (uint32_t j = out + lane; j < K; j += 32) row[j] = kEmpty;
+    upd += __reduce_add_sync(kFull, fresh_kept);
+    __syncwarp();
   }
   if (lane == 0) atomicAdd(&stats[2], upd);
 }
