@@ -162,6 +162,17 @@ def cpu_baseline(base, n_total, sample):
                       f"{sec:.2f}s measured, scaled by {n_total}/{sample}"}
 
 
+def workload_config(n, dim, world):
+    """The workload both arms report (the reference arm runs a bounded CPU sample of it)."""
+    return {"workload": "1M x 128 SIFT-like, GNN-Descent k=96 x10 + CFS path/dist 1.0 degree 32 "
+                        "m=64", "n": n, "dim": dim, "k": K, "iters": ITERS, "final_degree": FD,
+            "topm": TOPM, "storage": "f16 base",
+            "screen": "tcgen05 f16 Gram tiles, exact f32 re-rank of every kept pair",
+            "index_search": "reference NSG search, L=128, seeded random starts",
+            "l2": "inputs larger than L2 (512 MB FP32 + 256 MB FP16 base)",
+            "parallelism": f"replicas x{world}"}
+
+
 def reference_arm(a, rank):
     if rank != 0:
         return
@@ -180,9 +191,7 @@ def reference_arm(a, rank):
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": v * 1000.0,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic SIFT-like mixture (seeded), bounded CPU sample",
-            "config": {"workload": "1M x 128 SIFT-like, GNN-Descent k=96 x10 + CFS path/dist "
-                                   "1.0 degree 32 m=64", "n": a.n, "dim": 128, "k": K,
-                       "iters": ITERS, "final_degree": FD, "topm": TOPM},
+            "config": workload_config(a.n, 128, 1),
             "cpu_baseline": cb,
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -312,14 +321,7 @@ def main():
                 "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32",
                 "data": "synthetic SIFT-like mixture (seeded, 256 components)",
-                "config": {"workload": "1M x 128 SIFT-like, GNN-Descent k=96 x10 + CFS path/dist "
-                                       "1.0 degree 32 m=64", "n": n, "dim": dim, "k": K,
-                           "iters": ITERS, "final_degree": FD, "topm": TOPM,
-                           "storage": "f16 base", "screen": "tcgen05 f16 Gram tiles, exact f32 "
-                                                            "re-rank of every kept pair",
-                           "index_search": "reference NSG search, L=128, seeded random starts",
-                           "l2": "inputs larger than L2 (512 MB FP32 + 256 MB FP16 base)",
-                           "parallelism": f"replicas x{world}"},
+                "config": workload_config(n, dim, world),
                 "vectors_per_s": world * n / value,
                 "plain_fp32_s": plain_ms / 1000.0 if plain_ms else None,
                 "chosen_speedup_vs_plain": (plain_ms / ms) if plain_ms else None,

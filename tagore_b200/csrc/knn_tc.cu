@@ -1,6 +1,6 @@
 // knn_tc.cu -- local join on tcgen05 tensor cores (sm_100a).
 //
-// Persistent blocks (at most three per SM, so their three 128-column TMEM
+// Persistent blocks (three per SM, so their three 128-column TMEM
 // accumulators always fit in the SM's 512) walk the nodes. For each node's
 // join list (<= 128 FP16 rows):
 //   1. TMA tile::gather4 copies the rows into a K-major 128-byte-swizzled tile
@@ -12,11 +12,13 @@
 //      `per_row` closest partners that could beat the row's k-th entry
 //      (screened value below k-th + 2^-12 (n_r + n_c); the Gram entry's FP32
 //      accumulation error is below 2^-16 (n_r + n_c));
-//   4. each thread re-ranks its kept pairs exactly (reference-order FP32 from
-//      the same shared tile) and proposes a pair only when the exact value beats
-//      the k-th entry. No stored distance comes from a tensor core.
-// Two tile stages pipeline the loop: while node i is screened and re-ranked,
-// node i+1's rows are in flight and its MMA runs as soon as TMEM is free.
+//   4. the kept pairs of all rows are pooled and re-ranked exactly
+//      (reference-order FP32 from the same shared tile) by all threads; a pair
+//      is proposed only when the exact value beats the k-th entry. No stored
+//      distance comes from a tensor core.
+// A producer warp fills two tile stages: while node i is screened and
+// re-ranked, node i+1's rows are in flight, and its MMA goes into the single
+// accumulator as soon as the screen of node i has read it.
 // Every wait is bounded by %globaltimer; on expiry the block records an error,
 // waits (bounded) for its own copies and MMAs, frees its TMEM and returns.
 #include <cuda.h>
@@ -31,8 +33,8 @@ namespace {
 
 constexpr int kConsumers = 128;             // warps 0-3: one thread per tile row
 constexpr int kThreads = kConsumers + 32;    // warp 4: the producer
-constexpr int kStages = 3;                   // row tiles in flight
-constexpr uint32_t kTmemCols = 256;          // two 128-column accumulators
+constexpr int kStages = 2;                   // row tiles in flight
+constexpr uint32_t kTmemCols = 128;          // one 128-column accumulator
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
 constexpr uint32_t kDone = 0xFFFFFFFFu;      // stage node: the producer has finished
 constexpr float kOneMinusEps = 1.0f - 0.000244140625f;  // 1 - 2^-12, the screen's margin
@@ -269,12 +271,13 @@ __device__ void join_producer(TcSmem& s, const CUtensorMap& tmap, const uint64_t
 // Warp-specialised persistent join. The producer warp (join_producer) keeps
 // kStages nodes in flight; the four consumer warps take node i from stage
 // i % kStages: thread 0 has issued its Gram tile X X^T (tcgen05, M = N = 128,
-// K = 16 steps) into accumulator i % 2 one node earlier; every thread owns
-// one tile row, screens it from TMEM and re-ranks the kept pairs exactly.
-// Blocks of at most 114 KB of shared memory run at most two per SM, so their
-// 2 x 256 TMEM columns always fit.
+// K = 16 steps) into the block's accumulator right after the screen of node
+// i - 1; every thread owns one tile row, screens it from TMEM and re-ranks the
+// kept pairs exactly. Three blocks per SM (12 consumer warps) with one
+// 128-column accumulator each hide more latency than two blocks with two
+// accumulators each (240 against 312 ms for the 1M x 128 build's ten joins).
 template <int D>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 3)
     k_join_tc(const __grid_constant__ CUtensorMap tmap, const uint64_t* __restrict__ nb,
               const float* __restrict__ norms, const uint32_t* __restrict__ lists,
               const uint32_t* __restrict__ lcnt, uint32_t n, uint32_t dim, uint32_t K, uint32_t T,
@@ -342,7 +345,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     uint32_t got_full = 0;  // nodes whose rows this thread has seen land
     for (uint32_t i = 0;; ++i) {
       const int st = (int)(i % kStages);
-      const uint32_t acc = i & 1u;
+      const uint32_t acc = 0u;  // one accumulator, refilled once the screen has read it
       const bool got = mbar_wait_bounded(smem_u32(&s.full_bar[st]), ph_full[st]);
       ph_full[st] ^= 1u;
       got_full += got ? 1u : 0u;
@@ -408,12 +411,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane >= (uint32_t)o) incl += v;
       }
       if (lane == 31) s.warp_pairs[warp] = incl;
-      // accumulator acc ^ 1 was last read for node i - 1: node i + 1 may go in
+      // every consumer has read the accumulator: node i + 1's tile may go in
       asm volatile("tcgen05.fence::before_thread_sync;");
       consumers_sync();
       if (tid == 0) {
         const int st1 = (int)((i + 1) % kStages);
-        issue(st1, ph_full[st1], acc ^ 1u);  // the phase node i + 1 completes
+        issue(st1, ph_full[st1], 0u);  // the phase node i + 1 completes
       }
       uint32_t off = incl - kept, npairs = 0;
 #pragma unroll
@@ -493,16 +496,16 @@ int make_row_map(CUtensorMap* map, const __half* base, uint32_t n, uint32_t dim)
 
 template <int D>
 int launch(const Work& w, const CUtensorMap& map, cudaStream_t s) {
-  // More than a third of an SM's shared memory per block keeps residency at
-  // two blocks per SM, so their 2 x 256 TMEM columns always fit.
-  const size_t sm = std::max<size_t>(sizeof(TcSmem) + 1024, 80 * 1024);
+  // More than a quarter of an SM's shared memory per block keeps residency at
+  // three blocks per SM, so their 3 x 128 TMEM columns always fit.
+  const size_t sm = std::max<size_t>(sizeof(TcSmem) + 1024, 60 * 1024);
   TG_CUDA(cudaFuncSetAttribute((const void*)k_join_tc<D>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int* err = reinterpret_cast<int*>(w.stats + 4);
-  k_join_tc<D><<<sms * 2, kThreads, sm, s>>>(map, w.nb, w.norms, w.lists, w.lcnt, w.n, w.dim,
+  k_join_tc<D><<<sms * 3, kThreads, sm, s>>>(map, w.nb, w.norms, w.lists, w.lcnt, w.n, w.dim,
                                              w.K, w.T, w.P, w.pool, w.stats, err);
   TG_CUDA(cudaGetLastError());
   return TAGORE_OK;
