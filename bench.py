@@ -162,6 +162,17 @@ def cpu_baseline(base, n_total, sample):
                       f"{sec:.2f}s measured, scaled by {n_total}/{sample}"}
 
 
+def max_over_ranks(value, dist, device):
+    """The slowest rank's time: every rank takes part (the same collective on
+    every rank), and a single process returns its own value."""
+    if not dist:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload_config(n, dim, world):
     """The workload both arms report (the reference arm runs a bounded CPU sample of it)."""
     return {"workload": "1M x 128 SIFT-like, GNN-Descent k=96 x10 + CFS path/dist 1.0 degree 32 "
@@ -245,11 +256,7 @@ def main():
             e1.record(stream)
             torch.cuda.synchronize()
         capi.check(L.tagore_set_profiling(0))
-        ms = e0.elapsed_time(e1) / steps
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1) / steps, dist, "cuda")
         launches = capi.last_timings().kernel_launches
         return ms, stage_stats(capi), launches, clk.summary()
 
@@ -302,11 +309,7 @@ def main():
             t0 = time.perf_counter()
             capi.build_index_host(base, K, ITERS, FD, TOPM, THRE, out=out)
             ts.append(time.perf_counter() - t0)
-        e2e_s = statistics.mean(ts)
-        if dist:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+        e2e_s = max_over_ranks(statistics.mean(ts), dist, "cuda")
         e2e = {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(base.nbytes),
                "d2h_bytes_per_step": int(out.nbytes)}
 
