@@ -121,20 +121,18 @@ def recall_knn(g, half_t, samp, k=10):
 
 
 def index_recall(rows, ep, base, queries, half_t, k=10, L=128, seed=0x5EED):
-    """recall@10 of a fixed greedy search over the pruned rows: the reference's
-    NSG search (pool L, ep's neighbours plus seeded random starts)."""
+    """recall@10 of the library's GPU greedy search (tagore_search) over the
+    pruned rows: NSG's search with pool L, the entry point's neighbours plus
+    seeded random starts."""
     import torch
-    from oracle import oracle as orc
-    n = rows.shape[0]
-    deg = rows[:, 0].astype(np.int64)
-    offs = np.zeros(n + 1, np.uint64)
-    offs[1:] = np.cumsum(deg)
-    mask = np.arange(rows.shape[1] - 1)[None, :] < deg[:, None]
-    adj = rows[:, 1:][mask].astype(np.uint32)
-    x = base.astype(np.float32)
-    found = orc.greedy_search(x, offs, adj, ep, queries, L, k, seed)
-    xq = torch.as_tensor(queries, device=half_t.device)
-    xb = torch.as_tensor(x, device=half_t.device)
+    from tagore_b200 import capi
+    dev = half_t.device
+    offs, adj = capi.rows_to_csr(rows)
+    xb = torch.as_tensor(np.ascontiguousarray(base, np.float32), device=dev)
+    xq = torch.as_tensor(np.ascontiguousarray(queries, np.float32), device=dev)
+    found = capi.search(xb, torch.as_tensor(offs.astype(np.int64), device=dev),
+                        torch.as_tensor(adj.view(np.int32), device=dev), ep, xq, L, k,
+                        seed).cpu().numpy()
     d2 = (xq * xq).sum(1, keepdim=True) + (xb * xb).sum(1)[None] - 2.0 * (xq @ xb.T)
     truth = torch.topk(d2, k, largest=False).indices.cpu().numpy()
     return float(np.mean([len(set(found[i].tolist()) & set(truth[i].tolist())) / k

@@ -148,6 +148,47 @@ int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_
  * rows. */
 int tagore_connect(TagoreKnnState* st, uint32_t ep, uint64_t* added);
 
+/* Greedy search over a graph index, one query per warp: NSG's search
+ * (get_neighbors, src/common.cu:65-127) as the recall evaluator of built
+ * indexes. The pool holds L candidates sorted by squared L2 distance (ties:
+ * earlier arrival first); the first unexpanded one is expanded until none is
+ * left. It starts from the entry point's neighbours; with seed != 0 it then
+ * tops the pool up to L with seeded random nodes (splitmix64 draws), with
+ * seed == 0 the entry point itself goes first. */
+typedef struct TagoreSearchParams {
+  uint32_t L;         /* pool size */
+  uint32_t k;         /* ids written per query; slots past the pool get 0xFFFFFFFF */
+  uint64_t seed;      /* 0: entry point first; else seeded random starts */
+  uint32_t visit_cap; /* visited-set slots per query, rounded up to a power of two
+                         (0: 64 L, at least 16384); a query may visit half of them */
+  uint32_t pad_;
+} TagoreSearchParams;
+
+/* All pointers are on the current device: base (n x dim FP32), the graph as
+ * CSR (offs: n+1 u64, adj: `edges` u32; ids >= n are skipped), queries
+ * (nq x dim FP32) and out (nq x k u32). stream may be null (a private
+ * stream). Returns TAGORE_EINVAL when a query outgrows the visited set. */
+int tagore_search(const TagoreSearchParams* p, const float* base, uint64_t n, uint32_t dim,
+                  const uint64_t* offs, const uint32_t* adj, uint64_t edges, uint32_t ep,
+                  const float* queries, uint32_t nq, uint32_t* out, void* stream);
+
+/* Index readers, the inverse of the writers below: index_type is NSG, Vamana,
+ * NSSG, CAGRA or DPG (the strings Pruning takes, pybind.cu:177-221).
+ * tagore_index_info scans the file; tagore_index_read fills the CSR arrays
+ * (offs: n+1, adj: edges) for the n and edges it reported. */
+typedef struct TagoreIndexInfo {
+  uint64_t n;          /* nodes */
+  uint64_t edges;      /* adjacency entries over all nodes */
+  uint32_t max_degree; /* widest row */
+  uint32_t width;      /* header width (NSG, NSSG), max degree (Vamana), 0 (CAGRA, DPG) */
+  uint32_t n_eps;      /* entry points stored: NSG and Vamana 1, NSSG its count, else 0 */
+  uint32_t eps[16];    /* the first min(n_eps, 16) of them */
+  uint32_t pad_;
+} TagoreIndexInfo;
+int tagore_index_info(const char* path, const char* index_type, TagoreIndexInfo* info);
+int tagore_index_read(const char* path, const char* index_type, uint64_t n, uint64_t edges,
+                      uint64_t* offs, uint32_t* adj);
+
 /* cal_ep_gpu (src/Tagore_src.cu:1889-2058) alone: entry point of the graph
  * held in st (kNN rows) toward st->center. */
 int tagore_entry_point(TagoreKnnState* st, uint32_t topm, uint32_t* ep);

@@ -23,7 +23,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-ccbin", "/usr/bin/g++",
            "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]
-SOURCES = ["capi.cu", "prune.cu", "knn.cu", "knn_tc.cu", "mlp.cu", "connect.cu", "prep.cu",
+SOURCES = ["capi.cu", "prune.cu", "knn.cu", "knn_tc.cu", "mlp.cu", "connect.cu", "prep.cu", "search.cu",
            "io.cpp", "large_index.cpp"]
 
 

@@ -65,6 +65,17 @@ class ScreenStats(C.Structure):
                 ("last_best_kept", C.c_double)]
 
 
+class SearchParams(C.Structure):
+    _fields_ = [("L", C.c_uint32), ("k", C.c_uint32), ("seed", C.c_uint64),
+                ("visit_cap", C.c_uint32), ("pad_", C.c_uint32)]
+
+
+class IndexInfo(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("edges", C.c_uint64), ("max_degree", C.c_uint32),
+                ("width", C.c_uint32), ("n_eps", C.c_uint32), ("eps", C.c_uint32 * 16),
+                ("pad_", C.c_uint32)]
+
+
 class StageStat(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("ms", C.c_double), ("launches", C.c_uint64),
                 ("bytes", C.c_uint64), ("items", C.c_uint64)]
@@ -85,6 +96,12 @@ SIGNATURES = {
     "tagore_large_merge": (C.c_int, [C.POINTER(LargeParams), C.POINTER(C.c_void_p), C.c_void_p]),
     "tagore_entry_point": (C.c_int, [C.POINTER(KnnState), C.c_uint32, C.POINTER(C.c_uint32)]),
     "tagore_connect": (C.c_int, [C.POINTER(KnnState), C.c_uint32, C.POINTER(C.c_uint64)]),
+    "tagore_search": (C.c_int, [C.POINTER(SearchParams), C.c_void_p, C.c_uint64, C.c_uint32,
+                                C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p,
+                                C.c_uint32, C.c_void_p, C.c_void_p]),
+    "tagore_index_info": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(IndexInfo)]),
+    "tagore_index_read": (C.c_int, [C.c_char_p, C.c_char_p, C.c_uint64, C.c_uint64, C.c_void_p,
+                                    C.c_void_p]),
     "tagore_state_alloc": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(KnnState)]),
     "tagore_state_free": (C.c_int, [C.POINTER(KnnState)]),
     "tagore_state_upload": (C.c_int, [C.POINTER(KnnState), C.c_int, C.c_void_p, C.c_size_t]),
@@ -252,6 +269,55 @@ def connect(state, ep):
     added = C.c_uint64(0)
     check(lib().tagore_connect(C.byref(state.st), ep, C.byref(added)))
     return added.value
+
+
+def rows_to_csr(rows):
+    """[deg, ids...] rows (the pruned graph) as CSR: offs (n+1 u64), adj (u32)."""
+    rows = np.asarray(rows, dtype=np.uint32)
+    deg = rows[:, 0].astype(np.int64)
+    if np.any(deg >= rows.shape[1]):
+        raise ValueError("a row's degree exceeds its width")
+    offs = np.zeros(rows.shape[0] + 1, np.uint64)
+    offs[1:] = np.cumsum(deg)
+    mask = np.arange(rows.shape[1] - 1)[None, :] < deg[:, None]
+    return offs, np.ascontiguousarray(rows[:, 1:][mask], dtype=np.uint32)
+
+
+def search(base, offs, adj, ep, queries, L, k, seed=0, visit_cap=0, stream=None):
+    """Greedy search on the current CUDA device. base (n x dim f32), offs
+    (n+1 u64 as int64), adj (u32 as int32), queries (nq x dim f32) are CUDA
+    tensors; returns an nq x k int64 tensor of ids (-1 where the pool ran
+    short)."""
+    import torch
+    for t in (base, offs, adj, queries):
+        if not t.is_cuda or not t.is_contiguous():
+            raise ValueError("search takes contiguous CUDA tensors")
+    if base.dtype != torch.float32 or queries.dtype != torch.float32:
+        raise ValueError("base and queries are float32")
+    n, dim = base.shape
+    nq = queries.shape[0] if queries.numel() else 0
+    out = torch.empty((nq, k), dtype=torch.int32, device=base.device)
+    p = SearchParams(L, k, seed, visit_cap, 0)
+    check(lib().tagore_search(C.byref(p), base.data_ptr(), n, dim, offs.data_ptr(),
+                              adj.data_ptr(), adj.numel(), ep, queries.data_ptr(), nq,
+                              out.data_ptr(), stream))
+    return out.to(torch.int64) & 0xFFFFFFFF
+
+
+def index_info(path, index_type):
+    info = IndexInfo()
+    check(lib().tagore_index_info(str(path).encode(), index_type.encode(), C.byref(info)))
+    return info
+
+
+def index_read(path, index_type):
+    """Reads an index file back: (info, offs n+1 u64, adj u32)."""
+    info = index_info(path, index_type)
+    offs = np.zeros(info.n + 1, np.uint64)
+    adj = np.zeros(max(info.edges, 1), np.uint32)
+    check(lib().tagore_index_read(str(path).encode(), index_type.encode(), info.n, info.edges,
+                                  _ptr(offs), _ptr(adj)))
+    return info, offs, adj[:info.edges]
 
 
 def entry_point(state, topm=64):

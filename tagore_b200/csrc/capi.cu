@@ -494,6 +494,19 @@ int tagore_entry_point(TagoreKnnState* st, uint32_t topm, uint32_t* ep) {
   return stage_cal_ep(dev_of(st), topm, ep, s.s);
 }
 
+int tagore_search(const TagoreSearchParams* p, const float* base, uint64_t n, uint32_t dim,
+                  const uint64_t* offs, const uint32_t* adj, uint64_t edges, uint32_t ep,
+                  const float* queries, uint32_t nq, uint32_t* out, void* stream) {
+  if (!p) return fail(TAGORE_EINVAL, "null search parameters");
+  TG_TRY(search_check(*p, base, n, dim, offs, adj, edges, ep, queries, nq, out));
+  if (nq == 0) return TAGORE_OK;
+  if (stream) return greedy_search(*p, base, n, dim, offs, adj, edges, ep, queries, nq, out,
+                                   static_cast<cudaStream_t>(stream));
+  Stream s;
+  TG_TRY(s.init());
+  return greedy_search(*p, base, n, dim, offs, adj, edges, ep, queries, nq, out, s.s);
+}
+
 int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const char* mode,
                        const char* metric) {
   TG_TRY(check_prune(p, st));

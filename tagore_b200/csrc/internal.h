@@ -107,6 +107,16 @@ constexpr size_t kStaticScratchBytes = (size_t)16 << 20;
 int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
                      const std::string& metric, uint32_t* ep_host, cudaStream_t s);
 
+// ---- greedy search (search.cu) ----
+// tagore_search on stream s; device pointers throughout. search_check is its
+// argument validation alone (no device call).
+int search_check(const TagoreSearchParams& p, const float* base, uint64_t n, uint32_t dim,
+                 const uint64_t* offs, const uint32_t* adj, uint64_t edges, uint32_t ep,
+                 const float* queries, uint32_t nq, const uint32_t* out);
+int greedy_search(const TagoreSearchParams& p, const float* base, uint64_t n, uint32_t dim,
+                  const uint64_t* offs, const uint32_t* adj, uint64_t edges, uint32_t ep,
+                  const float* queries, uint32_t nq, uint32_t* out, cudaStream_t s);
+
 // ---- kNN graph (knn.cu) ----
 struct KnnArgs {
   uint32_t k, iters, mode;  // mode: TAGORE_KNN_CHOSEN / _PLAIN / _LEARNED

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "internal.h"
@@ -36,6 +37,93 @@ bool write_rows(File& out, const uint32_t* graph, uint32_t n, uint32_t k, uint64
     if (max_deg && gk > *max_deg) *max_deg = gk;
   }
   return true;
+}
+
+// Parses one of the five index layouts into CSR: a counting pass leaves offs
+// and adj null; a filling pass writes at most n_cap rows and e_cap ids.
+constexpr uint32_t kMaxRowDegree = 1u << 24;  // larger rows mean a corrupt file
+
+int read_index(const char* path, const char* type_c, TagoreIndexInfo* info, uint64_t n_cap,
+               uint64_t e_cap, uint64_t* offs, uint32_t* adj) {
+  if (!path || !type_c || !info) return fail(TAGORE_EINVAL, "index reader: null argument");
+  const std::string type(type_c);
+  const bool nsg = type == "NSG", vamana = type == "Vamana", nssg = type == "NSSG",
+             cagra = type == "CAGRA", dpg = type == "DPG";
+  if (!nsg && !vamana && !nssg && !cagra && !dpg)
+    return fail(TAGORE_EINVAL, "unknown index type '%s'", type_c);
+  File in(path, "rb");
+  if (!in.f) return fail(TAGORE_EIO, "cannot open '%s'", path);
+  auto rd = [&](void* p, size_t bytes) { return std::fread(p, 1, bytes, in.f) == bytes; };
+  TagoreIndexInfo r;
+  std::memset(&r, 0, sizeof(r));
+  uint64_t vamana_size = 0, dpg_rows = 0;
+  if (nsg || nssg) {
+    if (!rd(&r.width, 4)) return fail(TAGORE_EIO, "'%s': truncated header", path);
+    if (nsg) {
+      r.n_eps = 1;
+      if (!rd(&r.eps[0], 4)) return fail(TAGORE_EIO, "'%s': truncated header", path);
+    } else {
+      if (!rd(&r.n_eps, 4)) return fail(TAGORE_EIO, "'%s': truncated header", path);
+      for (uint32_t i = 0; i < r.n_eps; ++i) {
+        uint32_t e;
+        if (!rd(&e, 4)) return fail(TAGORE_EIO, "'%s': truncated entry points", path);
+        if (i < 16) r.eps[i] = e;
+      }
+    }
+  } else if (vamana) {
+    uint64_t frozen = 0;
+    r.n_eps = 1;
+    if (!rd(&vamana_size, 8) || !rd(&r.width, 4) || !rd(&r.eps[0], 4) || !rd(&frozen, 8))
+      return fail(TAGORE_EIO, "'%s': truncated header", path);
+  } else if (dpg) {
+    char magic[8];
+    uint32_t major = 0, minor = 0, cnt = 0;
+    if (!rd(magic, 8) || !rd(&major, 4) || !rd(&minor, 4) || !rd(&cnt, 4))
+      return fail(TAGORE_EIO, "'%s': truncated header", path);
+    if (std::memcmp(magic, "KNNGRAPH", 8) != 0) return fail(TAGORE_EIO, "'%s': not a KNNGRAPH file", path);
+    dpg_rows = cnt;
+  }
+  uint64_t n = 0, edges = 0;
+  if (offs) offs[0] = 0;
+  std::vector<uint32_t> row;
+  while (!dpg || n < dpg_rows) {
+    uint32_t deg = 0;
+    const size_t got = std::fread(&deg, 1, 4, in.f);
+    if (got == 0 && !dpg) break;  // end of the rows
+    if (got != 4) return fail(TAGORE_EIO, "'%s': truncated at row %llu", path, (unsigned long long)n);
+    if (dpg) {
+      uint32_t valid = 0;  // KGraph's second count; the row holds `deg` ids
+      if (!rd(&valid, 4)) return fail(TAGORE_EIO, "'%s': truncated at row %llu", path, (unsigned long long)n);
+    }
+    if (deg > kMaxRowDegree)
+      return fail(TAGORE_EIO, "'%s': row %llu claims %u ids", path, (unsigned long long)n, deg);
+    row.resize(deg);
+    if (!rd(row.data(), 4ull * deg))
+      return fail(TAGORE_EIO, "'%s': truncated at row %llu", path, (unsigned long long)n);
+    if (offs) {
+      if (n >= n_cap || edges + deg > e_cap)
+        return fail(TAGORE_EINVAL, "'%s': more rows or ids than the arrays hold", path);
+      std::memcpy(adj + edges, row.data(), 4ull * deg);
+      offs[n + 1] = edges + deg;
+    }
+    edges += deg;
+    if (deg > r.max_degree) r.max_degree = deg;
+    ++n;
+  }
+  if (vamana) {
+    const long long end = std::ftell(in.f);
+    if (end < 0 || (uint64_t)end != vamana_size)
+      return fail(TAGORE_EIO, "'%s': header size %llu, file holds %lld bytes", path,
+                  (unsigned long long)vamana_size, end);
+  }
+  if (offs && (n != n_cap || edges != e_cap))
+    return fail(TAGORE_EINVAL, "'%s': holds %llu rows and %llu ids, not %llu and %llu", path,
+                (unsigned long long)n, (unsigned long long)edges, (unsigned long long)n_cap,
+                (unsigned long long)e_cap);
+  r.n = n;
+  r.edges = edges;
+  *info = r;
+  return TAGORE_OK;
 }
 
 }  // namespace
@@ -81,6 +169,18 @@ int tagore_load_fvecs(const char* path, float* out, uint32_t n, uint32_t dim) {
     done += cnt;
   }
   return TAGORE_OK;
+}
+
+int tagore_index_info(const char* path, const char* index_type, TagoreIndexInfo* info) {
+  return read_index(path, index_type, info, 0, 0, nullptr, nullptr);
+}
+
+int tagore_index_read(const char* path, const char* index_type, uint64_t n, uint64_t edges,
+                      uint64_t* offs, uint32_t* adj) {
+  if (!offs || (!adj && edges)) return fail(TAGORE_EINVAL, "index reader: null output array");
+  TagoreIndexInfo info;
+  uint32_t dummy = 0;
+  return read_index(path, index_type, &info, n, edges, offs, adj ? adj : &dummy);
 }
 
 // StoreNSG (src/common.cu:151-162): [u32 width][u32 ep] then [deg][ids] rows.

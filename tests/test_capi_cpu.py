@@ -143,3 +143,83 @@ def test_tagore_module_surface():
         assert arg in doc
     with pytest.raises(ValueError):
         T.Pruning(8, 10, 4, 4, 8, (), "NSG")
+
+
+def csr_of_rows(g):
+    deg = g[:, 0].astype(np.int64)
+    offs = np.zeros(len(g) + 1, np.uint64)
+    offs[1:] = np.cumsum(deg)
+    return offs, np.concatenate([r[1:1 + r[0]] for r in g]).astype(np.uint32)
+
+
+@pytest.mark.parametrize("kind", ["NSG", "Vamana", "NSSG"])
+def test_index_reader_roundtrip_rows(capi, tmp_path, kind):
+    g = rows(64, 12, np.random.default_rng(5))
+    path = str(tmp_path / f"a.{kind}")
+    ptr = g.ctypes.data_as(C.c_void_p)
+    if kind == "NSG":
+        capi.check(capi.lib().tagore_store_nsg(path.encode(), ptr, 11, 9, 64, 12))
+    elif kind == "Vamana":
+        capi.check(capi.lib().tagore_store_vamana(path.encode(), ptr, 9, 64, 12))
+    else:
+        capi.check(capi.lib().tagore_store_nssg(path.encode(), ptr, 11, 64, 12))
+    info, offs, adj = capi.index_read(path, kind)
+    want_offs, want_adj = csr_of_rows(g)
+    assert info.n == 64 and info.edges == len(want_adj)
+    assert info.max_degree == int(g[:, 0].max())
+    assert np.array_equal(offs, want_offs) and np.array_equal(adj, want_adj)
+    if kind == "NSSG":
+        assert info.n_eps == 10 and len(set(info.eps[:10])) == 10
+    else:
+        assert info.n_eps == 1 and info.eps[0] == 9
+    assert info.width == (int(g[:, 0].max()) if kind == "Vamana" else 11)
+
+
+@pytest.mark.parametrize("kind", ["DPG", "CAGRA"])
+def test_index_reader_roundtrip_dense(capi, tmp_path, kind):
+    dense = np.random.default_rng(6).integers(0, 30, size=(30, 7)).astype(np.uint32)
+    path = str(tmp_path / f"a.{kind}")
+    fn = capi.lib().tagore_store_dpg if kind == "DPG" else capi.lib().tagore_store_cagra
+    capi.check(fn(path.encode(), dense.ctypes.data_as(C.c_void_p), 30, 7))
+    info, offs, adj = capi.index_read(path, kind)
+    assert (info.n, info.edges, info.max_degree, info.n_eps) == (30, 210, 7, 0)
+    assert np.array_equal(offs, np.arange(31, dtype=np.uint64) * 7)
+    assert np.array_equal(adj, dense.reshape(-1))
+
+
+def test_index_reader_errors(capi, tmp_path):
+    g = rows(20, 8, np.random.default_rng(7))
+    path = str(tmp_path / "a.vamana")
+    capi.check(capi.lib().tagore_store_vamana(path.encode(), g.ctypes.data_as(C.c_void_p), 0, 20, 8))
+    info = capi.IndexInfo()
+    L = capi.lib()
+    assert L.tagore_index_info(path.encode(), b"HNSW", C.byref(info)) == capi.TAGORE_EINVAL
+    assert L.tagore_index_info(b"/no/such/index", b"NSG", C.byref(info)) == capi.TAGORE_EIO
+    with open(path, "r+b") as f:                      # a row cut short
+        f.truncate(os.path.getsize(path) - 2)
+    assert L.tagore_index_info(path.encode(), b"Vamana", C.byref(info)) == capi.TAGORE_EIO
+    with open(path, "ab") as f:                       # whole rows, but the header's size is stale
+        f.write(b"\0\0")
+        f.write(struct.pack("<I", 0))
+    assert L.tagore_index_info(path.encode(), b"Vamana", C.byref(info)) == capi.TAGORE_EIO
+    dpg = str(tmp_path / "a.dpg")
+    open(dpg, "wb").write(b"KNNGRAPX" + struct.pack("<III", 2, 0, 0))
+    assert L.tagore_index_info(dpg.encode(), b"DPG", C.byref(info)) == capi.TAGORE_EIO
+    nsg = str(tmp_path / "b.nsg")
+    capi.check(L.tagore_store_nsg(nsg.encode(), g.ctypes.data_as(C.c_void_p), 8, 0, 20, 8))
+    info = capi.index_info(nsg, "NSG")
+    offs = np.zeros(info.n + 1, np.uint64)
+    adj = np.zeros(info.edges, np.uint32)
+    assert L.tagore_index_read(nsg.encode(), b"NSG", info.n - 1, info.edges,         # arrays too small
+                               offs.ctypes.data_as(C.c_void_p),
+                               adj.ctypes.data_as(C.c_void_p)) == capi.TAGORE_EINVAL
+
+
+def test_search_argument_checks_need_no_device(capi):
+    p = capi.SearchParams(16, 4, 0, 0, 0)
+    L = capi.lib()
+    # n = 0, and an entry point outside the base: rejected before any device call
+    assert L.tagore_search(C.byref(p), None, 0, 8, None, None, 0, 0, None, 0, None, None) == capi.TAGORE_EINVAL
+    assert L.tagore_search(C.byref(p), None, 5, 8, None, None, 0, 5, None, 1, None, None) == capi.TAGORE_EINVAL
+    # no queries: nothing to do
+    assert L.tagore_search(C.byref(p), None, 5, 8, None, None, 0, 0, None, 0, None, None) == capi.TAGORE_OK
