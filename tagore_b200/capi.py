@@ -241,6 +241,16 @@ def gnn_descent_host(data, k, iters, mode=KNN_CHOSEN, rescale=1, seed=0x7A6E, sa
     return s
 
 
+def gnn_descent_file(path, k, iters, mode=KNN_CHOSEN, rescale=1, seed=0x7A6E):
+    """GNN_descent from an fvecs file; the file is parsed on the device."""
+    n, dim = C.c_uint32(), C.c_uint32()
+    check(lib().tagore_load_fvecs_header(str(path).encode(), C.byref(n), C.byref(dim)))
+    p = knn_params(k, n.value, dim.value, iters, mode, 0, 0, rescale, seed)
+    s = State()
+    check(lib().tagore_gnn_descent(C.byref(p), str(path).encode(), C.byref(s.st)))
+    return s
+
+
 def pruning(state, final_degree, index_type, topm=64, thre=1.0, index_path=None):
     st = state.st
     p = PruneParams(st.k, st.n, st.dim, final_degree, topm, thre)

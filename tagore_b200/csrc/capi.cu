@@ -240,15 +240,23 @@ int check_prune(const TagorePruneParams* p, TagoreKnnState* st) {
   return TAGORE_OK;
 }
 
+// Builds the state from the FP32 base on the device. The factor and the
+// centroid come from host_for_center (the same base in host memory, summed on
+// host threads while the device works); with host_for_center null they come
+// from `factor` and the device's own sequential centroid.
 int build_from_device(const TagoreKnnParams* p, const float* raw_dev, const float* host_for_center,
-                      uint32_t n, uint32_t dim, TagoreKnnState* st, cudaStream_t s) {
+                      float factor, uint32_t n, uint32_t dim, TagoreKnnState* st, cudaStream_t s) {
   const bool rescale = p->rescale != 0;
-  st->norm_factor = host_factor(host_for_center, dim, rescale);
+  st->norm_factor = host_for_center ? host_factor(host_for_center, dim, rescale) : factor;
   Timer t0;
   t0.start(s);
   TG_TRY(prep_base(raw_dev, n, dim, st->norm_factor, (__half*)st->data, (float*)st->norms, s));
   std::vector<uint16_t> center(dim);
-  std::thread cth(host_center, host_for_center, n, dim, st->norm_factor, center.data());
+  std::thread cth;
+  if (host_for_center)
+    cth = std::thread(host_center, host_for_center, n, dim, st->norm_factor, center.data());
+  else
+    TG_TRY(device_center(raw_dev, n, dim, st->norm_factor, (__half*)st->center, s));
   KnnArgs a{p->k,       p->iters, p->mode,        p->sample,
             p->per_row, p->seed,  p->learn_steps, p->learn_flags};
   KnnStats ks{};
@@ -256,12 +264,13 @@ int build_from_device(const TagoreKnnParams* p, const float* raw_dev, const floa
   const int rc = knn_build(dev_of(st), (const float*)st->norms, a, &ks, s);
   g_times.knn_ms = t0.stop(s);
   const auto w1 = std::chrono::steady_clock::now();
-  cth.join();
+  if (cth.joinable()) cth.join();
   const auto w2 = std::chrono::steady_clock::now();
   g_times.prep_ms = std::chrono::duration<double, std::milli>(w2 - w1).count();  // centroid wait
   g_times.total_ms = std::chrono::duration<double, std::milli>(w2 - w0).count();
   TG_TRY(rc);
-  TG_CUDA(cudaMemcpyAsync(st->center, center.data(), (size_t)dim * 2, cudaMemcpyHostToDevice, s));
+  if (host_for_center)
+    TG_CUDA(cudaMemcpyAsync(st->center, center.data(), (size_t)dim * 2, cudaMemcpyHostToDevice, s));
   TG_CUDA(cudaStreamSynchronize(s));
   return TAGORE_OK;
 }
@@ -447,7 +456,7 @@ int tagore_gnn_descent_host(const TagoreKnnParams* p, const float* data, uint32_
   }
   const cudaError_t e = cudaMemcpyAsync(raw, data, (size_t)n * dim * 4, cudaMemcpyHostToDevice, st.s);
   if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpyAsync(raw)", __FILE__, __LINE__);
-  if (rc == TAGORE_OK) rc = build_from_device(p, raw, data, n, dim, out, st.s);
+  if (rc == TAGORE_OK) rc = build_from_device(p, raw, data, 1.0f, n, dim, out, st.s);
   pool_free(raw, st.s);
   cudaStreamSynchronize(st.s);
   if (rc != TAGORE_OK) tagore_state_free(out);
@@ -464,19 +473,34 @@ int tagore_gnn_descent_device(const TagoreKnnParams* p, const float* dev_data,
   Stream st;
   TG_TRY(st.init());
   TG_TRY(tagore_state_alloc(n, dim, p->k, out));
-  const int rc = build_from_device(p, dev_data, host_data, n, dim, out, st.s);
+  const int rc = build_from_device(p, dev_data, host_data, 1.0f, n, dim, out, st.s);
   if (rc != TAGORE_OK) tagore_state_free(out);
   return rc;
 }
 
+// GNN_descent's file path (pybind.cu:19-105) with the parsing on the device:
+// the file streams through pinned chunks, the device strips each record's
+// count and checks it, and the factor, FP16 base, norms and centroid are made
+// on the device.
 int tagore_gnn_descent(const TagoreKnnParams* p, const char* fvecs_path, TagoreKnnState* out) {
   if (!p || !fvecs_path || !out) return fail(TAGORE_EINVAL, "null argument");
   uint32_t n = 0, dim = 0;
   TG_TRY(tagore_load_fvecs_header(fvecs_path, &n, &dim));
   if (dim != p->dim) return fail(TAGORE_EINVAL, "file DIM %u differs from DIM %u", dim, p->dim);
-  std::vector<float> host((size_t)n * dim);
-  TG_TRY(tagore_load_fvecs(fvecs_path, host.data(), n, dim));
-  return tagore_gnn_descent_host(p, host.data(), n, dim, out);
+  if (dim % 4) return fail(TAGORE_EINVAL, "DIM must be a multiple of 4 (got %u)", dim);
+  if (p->k == 0 || p->k >= n) return fail(TAGORE_EINVAL, "need POINTS > K >= 1");
+  Stream st;
+  TG_TRY(st.init());
+  TG_TRY(tagore_state_alloc(n, dim, p->k, out));
+  float* raw = nullptr;
+  float factor = 1.0f;
+  int rc = pool_alloc((void**)&raw, (size_t)n * dim * 4, st.s);
+  if (rc == TAGORE_OK) rc = ingest_fvecs(fvecs_path, n, dim, p->rescale != 0, raw, &factor, st.s);
+  if (rc == TAGORE_OK) rc = build_from_device(p, raw, nullptr, factor, n, dim, out, st.s);
+  if (raw) pool_free(raw, st.s);
+  cudaStreamSynchronize(st.s);
+  if (rc != TAGORE_OK) tagore_state_free(out);
+  return rc;
 }
 
 int tagore_connect(TagoreKnnState* st, uint32_t ep, uint64_t* added) {

@@ -157,5 +157,12 @@ int prep_base(const float* raw, uint32_t n, uint32_t dim, float factor, __half* 
               cudaStream_t s);
 float host_factor(const float* x, uint32_t dim, bool rescale);
 void host_center(const float* x, uint32_t n, uint32_t dim, float factor, uint16_t* center_half);
+// The same centroid on the device from raw (n x dim FP32 on the device).
+int device_center(const float* raw, uint32_t n, uint32_t dim, float factor, __half* center,
+                  cudaStream_t s);
+// fvecs file -> raw (n x dim FP32 on the device) through pinned chunks;
+// *factor = host_factor of vector 0.
+int ingest_fvecs(const char* path, uint32_t n, uint32_t dim, bool rescale, float* raw,
+                 float* factor, cudaStream_t s);
 
 }  // namespace tagore
