@@ -17,31 +17,57 @@ __device__ __forceinline__ float2 h2lo(uint32_t v) {
   return __half22float2(*reinterpret_cast<const __half2*>(&v));
 }
 
+// Packed FP32 pair arithmetic of sm_100 (PTX .f32x2): each half is its own
+// IEEE operation rounded to nearest, so a pair op equals the two scalar ops.
+// (x, y) += (a, b), and (x, y) = (d0*d0 + x, d1*d1 + y).
+__device__ __forceinline__ void add2(float& x, float& y, float a, float b) {
+  asm("{.reg .b64 p, q;\n\t"
+      "mov.b64 p, {%0, %1};\n\t"
+      "mov.b64 q, {%2, %3};\n\t"
+      "add.rn.f32x2 p, p, q;\n\t"
+      "mov.b64 {%0, %1}, p;}"
+      : "+f"(x), "+f"(y)
+      : "f"(a), "f"(b));
+}
+__device__ __forceinline__ void fma2_sq(float& x, float& y, float d0, float d1) {
+  asm("{.reg .b64 p, q;\n\t"
+      "mov.b64 p, {%0, %1};\n\t"
+      "mov.b64 q, {%2, %3};\n\t"
+      "fma.rn.f32x2 p, q, q, p;\n\t"
+      "mov.b64 {%0, %1}, p;}"
+      : "+f"(x), "+f"(y)
+      : "f"(d0), "f"(d1));
+}
+// (d0, d1) = (float(a.lo) - b0, float(a.hi) - b1), one rounding each: the
+// mixed f16/f32 subtract widens a exactly, as __half2float would.
+__device__ __forceinline__ void sub_h2(uint32_t a, float b0, float b1, float& d0, float& d1) {
+  asm("{.reg .b16 lo, hi;\n\t"
+      "mov.b32 {lo, hi}, %2;\n\t"
+      "sub.rn.f32.f16 %0, lo, %3;\n\t"
+      "sub.rn.f32.f16 %1, hi, %4;}"
+      : "=f"(d0), "=f"(d1)
+      : "r"(a), "f"(b0), "f"(b1));
+}
+
 // Accumulates one 4-dim chunk into the lane's (x, y) pair exactly as the
 // reference's two __hfma2 steps do (src/Tagore_src.cu:1431-1435), in FP32:
 // x takes dims 0 and 2, y takes dims 1 and 3, each a fused multiply-add of the
 // rounded difference.
 __device__ __forceinline__ void chunk_acc(uint2 a, uint2 b, float& x, float& y) {
-  const float2 a01 = h2lo(a.x), a23 = h2lo(a.y);
   const float2 b01 = h2lo(b.x), b23 = h2lo(b.y);
-  const float d0 = __fsub_rn(a01.x, b01.x);
-  const float d1 = __fsub_rn(a01.y, b01.y);
-  const float d2 = __fsub_rn(a23.x, b23.x);
-  const float d3 = __fsub_rn(a23.y, b23.y);
-  x = __fmaf_rn(d0, d0, x);
-  y = __fmaf_rn(d1, d1, y);
-  x = __fmaf_rn(d2, d2, x);
-  y = __fmaf_rn(d3, d3, y);
+  float d0, d1, d2, d3;
+  sub_h2(a.x, b01.x, b01.y, d0, d1);
+  sub_h2(a.y, b23.x, b23.y, d2, d3);
+  fma2_sq(x, y, d0, d1);
+  fma2_sq(x, y, d2, d3);
 }
 
 // Reduces the per-lane pairs with the reference's shuffle-down tree (offsets
 // 16..1) and returns x + y in every lane.
 __device__ __forceinline__ float warp_tree(float x, float y) {
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    x = __fadd_rn(x, __shfl_down_sync(kFull, x, off));
-    y = __fadd_rn(y, __shfl_down_sync(kFull, y, off));
-  }
+  for (int off = 16; off > 0; off >>= 1)
+    add2(x, y, __shfl_down_sync(kFull, x, off), __shfl_down_sync(kFull, y, off));
   return __shfl_sync(kFull, __fadd_rn(x, y), 0);
 }
 
@@ -79,10 +105,8 @@ __device__ __forceinline__ void warp_dist4(const __half* __restrict__ q, const _
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      x[t] = __fadd_rn(x[t], __shfl_down_sync(kFull, x[t], off));
-      y[t] = __fadd_rn(y[t], __shfl_down_sync(kFull, y[t], off));
-    }
+    for (int t = 0; t < 4; ++t)
+      add2(x[t], y[t], __shfl_down_sync(kFull, x[t], off), __shfl_down_sync(kFull, y[t], off));
   }
 #pragma unroll
   for (int t = 0; t < 4; ++t) out[t] = __shfl_sync(kFull, __fadd_rn(x[t], y[t]), 0);
@@ -103,8 +127,9 @@ __device__ __forceinline__ void lane_tree(Leaf& leaf, float& x, float& y) {
     float ax, ay, bx, by;
     lane_tree<Level - 1, Slot>(leaf, ax, ay);
     lane_tree<Level - 1, Slot + (32 >> Level)>(leaf, bx, by);
-    x = __fadd_rn(ax, bx);
-    y = __fadd_rn(ay, by);
+    add2(ax, ay, bx, by);
+    x = ax;
+    y = ay;
   }
 }
 
@@ -149,10 +174,12 @@ __device__ __forceinline__ void level2_pair(Load16& load, int p, float (&x)[2], 
   // level 2 pairs the two results.
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    const float ax = __fadd_rn(lx[0][h], lx[2][h]), ay = __fadd_rn(ly[0][h], ly[2][h]);
-    const float bx = __fadd_rn(lx[1][h], lx[3][h]), by = __fadd_rn(ly[1][h], ly[3][h]);
-    x[h] = __fadd_rn(ax, bx);
-    y[h] = __fadd_rn(ay, by);
+    float ax = lx[0][h], ay = ly[0][h], bx = lx[1][h], by = ly[1][h];
+    add2(ax, ay, lx[2][h], ly[2][h]);
+    add2(bx, by, lx[3][h], ly[3][h]);
+    add2(ax, ay, bx, by);
+    x[h] = ax;
+    y[h] = ay;
   }
 }
 
@@ -164,13 +191,14 @@ __device__ __forceinline__ float dist128_pairs(Load16 load) {
   level2_pair(load, 1, x1, y1);  // 2, 3
   level2_pair(load, 3, x3, y3);  // 6, 7
   // level 3: m + m+4; level 4: m + m+2; level 5: 0 + 1
-  const float x30 = __fadd_rn(x0[0], x2[0]), y30 = __fadd_rn(y0[0], y2[0]);
-  const float x31 = __fadd_rn(x0[1], x2[1]), y31 = __fadd_rn(y0[1], y2[1]);
-  const float x32 = __fadd_rn(x1[0], x3[0]), y32 = __fadd_rn(y1[0], y3[0]);
-  const float x33 = __fadd_rn(x1[1], x3[1]), y33 = __fadd_rn(y1[1], y3[1]);
-  const float x40 = __fadd_rn(x30, x32), y40 = __fadd_rn(y30, y32);
-  const float x41 = __fadd_rn(x31, x33), y41 = __fadd_rn(y31, y33);
-  return __fadd_rn(__fadd_rn(x40, x41), __fadd_rn(y40, y41));
+  add2(x0[0], y0[0], x2[0], y2[0]);
+  add2(x0[1], y0[1], x2[1], y2[1]);
+  add2(x1[0], y1[0], x3[0], y3[0]);
+  add2(x1[1], y1[1], x3[1], y3[1]);
+  add2(x0[0], y0[0], x1[0], y1[0]);
+  add2(x0[1], y0[1], x1[1], y1[1]);
+  add2(x0[0], y0[0], x0[1], y0[1]);
+  return __fadd_rn(x0[0], y0[0]);
 }
 
 __device__ __forceinline__ float row_dist128(const __half* __restrict__ a,
