@@ -35,6 +35,10 @@ __device__ __forceinline__ uint32_t align4(uint32_t x) { return (x + 3u) & ~3u; 
 // ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
 // Beam search shared by cal_ep_gpu (:1905-2047) and collect_path (:1211-1335).
+// The helpers below are __noinline__: the select kernel is latency-bound and
+// its warps sit in different phases, so one copy of each sort and merge keeps
+// the code they run small enough for the instruction cache (inlined copies
+// at every call site cost 8 % of the select at 1M points).
 struct Beam {
   uint32_t* id;
   float* dis;
@@ -76,7 +80,7 @@ __device__ __forceinline__ uint32_t hslot(uint32_t key, uint32_t mask) {
 // The reference keeps the beam ids sorted (top_M_Cand2, :1253-1259) only to
 // test membership (:1282-1290); a hash set of the same ids answers the same
 // question without a sort.
-__device__ void beam_rehash(Beam bm, uint32_t W, int lane) {
+__device__ __noinline__ void beam_rehash(Beam bm, uint32_t W, int lane) {
   for (uint32_t t = lane; t <= bm.hmask; t += 32) bm.hash[t] = kInv;
   __syncwarp();
   for (uint32_t t = lane; t < W; t += 32) {
@@ -102,7 +106,7 @@ __device__ __forceinline__ bool beam_has(const Beam& bm, uint32_t key) {
   }
 }
 
-__device__ void beam_network(Beam bm, uint32_t off, uint32_t len, int lane) {
+__device__ __noinline__ void beam_network(Beam bm, uint32_t off, uint32_t len, int lane) {
   float* D = bm.dis + off;
   uint32_t* I = bm.id + off;
   uint8_t* E = bm.ex + off;
@@ -132,7 +136,7 @@ __device__ __forceinline__ float key_dis(uint64_t k) { return __uint_as_float((u
 // [0, m), into the sorted prefix [0, topm) by rank, through the staging
 // arrays. Returns false (nothing moved) when two merged positions 0..topm tie.
 template <int E>
-__device__ bool beam_merge(Beam bm, uint32_t topm, uint32_t m, int lane) {
+__device__ __noinline__ bool beam_merge(Beam bm, uint32_t topm, uint32_t m, int lane) {
   uint64_t key[E];
 #pragma unroll
   for (int t = 0; t < E; ++t) {
@@ -204,7 +208,7 @@ __device__ bool beam_merge(Beam bm, uint32_t topm, uint32_t m, int lane) {
 // correct sort. With a full prefix only scored entries no farther than its
 // last one can reach positions 0..topm, so just those are sorted and merged
 // by rank; a tie there, or a prefix that is not full, runs the network.
-__device__ void beam_update(Beam bm, uint32_t topm, uint32_t K, const uint32_t* fresh,
+__device__ __noinline__ void beam_update(Beam bm, uint32_t topm, uint32_t K, const uint32_t* fresh,
                             uint32_t nfresh, int lane) {
   const uint32_t W = topm + K;
   beam_rehash(bm, W, lane);  // the set of all W ids, before anything moves
@@ -377,7 +381,7 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
 
 // Sort by distance with the reference network, then mark adjacent repeats
 // using the ids as they were before marking (:1345-1348).
-__device__ void warp_sort_mark(uint32_t* cand, float* dis, uint32_t len, int lane) {
+__device__ __noinline__ void warp_sort_mark(uint32_t* cand, float* dis, uint32_t len, int lane) {
   warp_network(len, lane, [&](uint32_t u, uint32_t d) { return dis[u] > dis[d]; },
                [&](uint32_t u, uint32_t d) {
                  swap_(dis[u], dis[d]);
