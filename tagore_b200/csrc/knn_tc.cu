@@ -122,6 +122,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// (v0, v1) = (-2 g0 + h0, -2 g1 + h1) as one packed FP32 pair FMA (each half
+// rounded once, as fmaf).
+__device__ __forceinline__ void fma2_m2(float g0, float g1, float h0, float h1, float& v0,
+                                        float& v1) {
+  asm("{.reg .b64 a, b, c;\n\t"
+      "mov.b64 a, {%2, %3};\n\t"
+      "mov.b64 b, {%6, %6};\n\t"
+      "mov.b64 c, {%4, %5};\n\t"
+      "fma.rn.f32x2 c, a, b, c;\n\t"
+      "mov.b64 {%0, %1}, c;}"
+      : "=f"(v0), "=f"(v1)
+      : "f"(g0), "f"(g1), "f"(h0), "f"(h1), "f"(-2.0f));
+}
+
 // Chunk j (4 halves) of row r inside a swizzled tile.
 __device__ __forceinline__ uint2 tile_chunk(const Tile& t, uint32_t r, uint32_t j) {
   const uint32_t blk = j >> 4, unit = ((j & 15u) >> 1) ^ (r & 7u), half8 = j & 1u;
@@ -379,24 +393,35 @@ __global__ void __launch_bounds__(kThreads, 3)
       // the warp reads only the column blocks one of its rows needs
       const uint32_t cmax = live ? ((r < nn) ? total : nn) : 0u;
       const uint32_t wmax = __reduce_max_sync(kFull, cmax);
+      // cut = min(lim, the row's current T-th kept value), refreshed only when
+      // a pair is kept; a column takes the insertion branch only below it
+      float cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
 #pragma unroll 1
       for (uint32_t q = 0; q * 32 < wmax; ++q) {
         float g[32];
         tmem_ld32(tmem + acc * 128 + ((warp * 32u) << 16) + q * 32u, g);
+        if (q * 32 >= cmax) continue;  // no column of this block pairs with row r
+        const float4* h4 = reinterpret_cast<const float4*>(&s.hnrm[st][q * 32]);
 #pragma unroll
-        for (int k = 0; k < 32; ++k) {
-          const uint32_t c = q * 32 + k;
-          const float v0 = fmaf(-2.0f, g[k], s.hnrm[st][c]);
-          const float worst = T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3]));
-          if (v0 < lim && v0 < worst && c < cmax && c != r) {
-            float v = v0;
-            uint32_t vc = c;
+        for (int k4 = 0; k4 < 8; ++k4) {
+          const float4 h = h4[k4];
+          float v4[4];
+          fma2_m2(g[4 * k4], g[4 * k4 + 1], h.x, h.y, v4[0], v4[1]);
+          fma2_m2(g[4 * k4 + 2], g[4 * k4 + 3], h.z, h.w, v4[2], v4[3]);
 #pragma unroll
-            for (int t = 0; t < 4; ++t)
-              if (v < bd[t]) {
-                swap_(v, bd[t]);
-                swap_(vc, bc[t]);
-              }
+          for (int j = 0; j < 4; ++j) {
+            const uint32_t c = q * 32 + 4 * k4 + j;
+            if (v4[j] < cut && c < cmax && c != r) {
+              float v = v4[j];
+              uint32_t vc = c;
+#pragma unroll
+              for (int t = 0; t < 4; ++t)
+                if (v < bd[t]) {
+                  swap_(v, bd[t]);
+                  swap_(vc, bc[t]);
+                }
+              cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
+            }
           }
         }
       }
