@@ -295,22 +295,35 @@ __global__ void __launch_bounds__(128)
   for (uint32_t u = blockIdx.x * 4 + warp; u < n; u += gridDim.x * 4) {
     uint64_t* row = nb + (size_t)u * K;
     unsigned long long* pl = pool + (size_t)u * P;
+    // the k-th key, the pool and the row are loaded together: one round trip
     const uint64_t kth = row[K - 1];
+    uint64_t pk[kPool / 32], rk[kMaxList / 32];
+#pragma unroll
+    for (int t = 0; t < (int)(kPool / 32); ++t) {
+      const uint32_t j = 32 * t + lane;
+      pk[t] = j < P ? (uint64_t)pl[j] : kEmpty;
+    }
+#pragma unroll
+    for (int t = 0; t < (int)(kMaxList / 32); ++t) {
+      const uint32_t j = 32 * t + lane;
+      rk[t] = j < K ? row[j] : kEmpty;
+    }
     uint32_t m = 0;
-    for (uint32_t base = 0; base < P; base += 32) {
-      const uint32_t j = base + lane;
-      uint64_t k = kEmpty;
-      if (j < P) {
-        k = pl[j];
-        if (k != kEmpty) pl[j] = kEmpty;
-      }
+#pragma unroll
+    for (int t = 0; t < (int)(kPool / 32); ++t) {
+      const uint64_t k = pk[t];
+      if (k != kEmpty) pl[32 * t + lane] = kEmpty;
       const bool fresh = k < kth;
       const unsigned mk = __ballot_sync(kFull, fresh);
       if (fresh) fb[m + __popc(mk & lt)] = k;
       m += __popc(mk);
     }
     if (m == 0) continue;
-    for (uint32_t j = lane; j < K; j += 32) rb[j] = row[j];
+#pragma unroll
+    for (int t = 0; t < (int)(kMaxList / 32); ++t) {
+      const uint32_t j = 32 * t + lane;
+      if (j < K) rb[j] = rk[t];
+    }
     __syncwarp();
     if (m <= 32) sort_fresh<1>(fb, m, lane);
     else if (m <= 64) sort_fresh<2>(fb, m, lane);
