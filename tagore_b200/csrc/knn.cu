@@ -58,18 +58,13 @@ __global__ void __launch_bounds__(128)
         keys[t] = (uint64_t)v;
       }
     }
-    for (int t = 0; t < 4; ++t) {
-      for (int l0 = 0; l0 < 32; l0 += 4) {
-        uint32_t ids[4];
-        float d4[4];
+    // one neighbour row per lane, in the reference's lane order (row_dist)
+    const __half* q = data + (size_t)u * dim;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const uint64_t k = shfl_u64(keys[t], l0 + q);
-          ids[q] = (k == kEmpty) ? kInv : (uint32_t)k;
-        }
-        warp_dist4(data + (size_t)u * dim, data, dim, ids, d4, lane);
-        const int q = lane - l0;
-        if (q >= 0 && q < 4 && keys[t] != kEmpty) keys[t] = make_key(d4[q], (uint32_t)keys[t], true);
+    for (int t = 0; t < 4; ++t) {
+      if (keys[t] != kEmpty) {
+        const uint32_t v = (uint32_t)keys[t];
+        keys[t] = make_key(row_dist(q, data + (size_t)v * dim, dim), v, true);
       }
     }
     warp_sort_keys<4>(keys, lane);
