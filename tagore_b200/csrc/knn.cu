@@ -124,51 +124,40 @@ __global__ void __launch_bounds__(128)
                   const uint32_t* __restrict__ rnew, const uint32_t* __restrict__ rold,
                   const uint32_t* __restrict__ rcnt, uint32_t* __restrict__ lists,
                   uint32_t* __restrict__ lcnt) {
-  __shared__ uint32_t raw_all[4][4 * kMaxS];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  uint32_t* raw = raw_all[warp];
   for (uint32_t u = blockIdx.x * 4 + warp; u < n; u += gridDim.x * 4) {
-    const uint32_t a = fcnt[2 * u], b = min(rcnt[2 * u], S);
-    const uint32_t c = fcnt[2 * u + 1], e = min(rcnt[2 * u + 1], S);
-    const uint32_t nraw = a + b, total_raw = a + b + c + e;
-    for (uint32_t i = lane; i < total_raw; i += 32) {
-      uint32_t v;
-      if (i < a) v = fnew[(size_t)u * S + i];
-      else if (i < a + b) v = rnew[(size_t)u * S + (i - a)];
-      else if (i < a + b + c) v = fold[(size_t)u * S + (i - a - b)];
-      else v = rold[(size_t)u * S + (i - a - b - c)];
-      raw[i] = v;
-    }
-    __syncwarp();
-    uint32_t keep_mask[4];
+    // the four sources, one entry per lane (S <= 32): forward new, reverse
+    // new, forward old, reverse old -- the order in which repeats keep their
+    // first copy
+    const uint32_t cnt[4] = {fcnt[2 * u], min(rcnt[2 * u], S), fcnt[2 * u + 1],
+                             min(rcnt[2 * u + 1], S)};
+    const uint32_t* src[4] = {fnew, rnew, fold, rold};
+    uint32_t x[4];
 #pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const uint32_t i = lane + 32 * t;
-      bool keep = false;
-      if (i < total_raw) {
-        const uint32_t v = raw[i];
-        keep = v != u;
-        for (uint32_t j = 0; j < i && keep; ++j) keep = raw[j] != v;
-      }
-      keep_mask[t] = keep ? 1u : 0u;
+    for (int q = 0; q < 4; ++q)
+      x[q] = (uint32_t)lane < cnt[q] ? src[q][(size_t)u * S + lane] : kInv;
+    // an entry is kept when it is not u and no earlier entry holds its id:
+    // earlier lanes of its own source (match), then every earlier source
+    bool keep[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const unsigned same = __match_any_sync(kFull, x[q]);
+      bool dup = (same & lt) != 0u;
+#pragma unroll
+      for (int q2 = 0; q2 < q; ++q2)
+        for (uint32_t j = 0; j < cnt[q2]; ++j) dup |= __shfl_sync(kFull, x[q2], j) == x[q];
+      keep[q] = (uint32_t)lane < cnt[q] && x[q] != u && !dup;
     }
-    // ordered compaction: kept new entries first, then kept old entries
     uint32_t pos = 0;
-    for (int pass = 0; pass < 2; ++pass) {
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        const uint32_t i = lane + 32 * t;
-        const bool in_pass = pass == 0 ? (i < nraw) : (i >= nraw && i < total_raw);
-        const bool k = keep_mask[t] && in_pass;
-        const unsigned m = __ballot_sync(kFull, k);
-        if (k) lists[(size_t)u * kMaxList + pos + __popc(m & lt)] = raw[i];
-        pos += __popc(m);
-      }
-      if (pass == 0 && lane == 0) lcnt[2 * u] = pos;
+    for (int q = 0; q < 4; ++q) {
+      const unsigned m = __ballot_sync(kFull, keep[q]);
+      if (keep[q]) lists[(size_t)u * kMaxList + pos + __popc(m & lt)] = x[q];
+      pos += __popc(m);
+      if (q == 1 && lane == 0) lcnt[2 * u] = pos;  // the new entries
     }
     if (lane == 0) lcnt[2 * u + 1] = pos;
-    __syncwarp();
   }
 }
 
