@@ -201,6 +201,49 @@ __device__ __forceinline__ float dist128_pairs(Load16 load) {
   return __fadd_rn(x0[0], y0[0]);
 }
 
+// The same tree for any width that is a multiple of 8 halves (`units`
+// 16-byte units): lane slot s accumulates chunks s, s + 32, ... in order, so
+// the leaves of pair p + 4q are summed over the units p + 4q, p + 4q + 16, ...
+// before the level-1 and level-2 combining above. At 128 dims there is one
+// round and this is dist128_pairs.
+template <class Load16>
+__device__ __forceinline__ void level2_pair_rounds(Load16& load, int p, uint32_t units,
+                                                   float (&x)[2], float (&y)[2]) {
+  float lx[4][2], ly[4][2];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    lx[q][0] = ly[q][0] = lx[q][1] = ly[q][1] = 0.0f;
+    for (uint32_t u = p + 4 * q; u < units; u += 16)
+      pair_acc(load(u, 0), load(u, 1), lx[q][0], ly[q][0], lx[q][1], ly[q][1]);
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float ax = lx[0][h], ay = ly[0][h], bx = lx[1][h], by = ly[1][h];
+    add2(ax, ay, lx[2][h], ly[2][h]);
+    add2(bx, by, lx[3][h], ly[3][h]);
+    add2(ax, ay, bx, by);
+    x[h] = ax;
+    y[h] = ay;
+  }
+}
+
+template <class Load16>
+__device__ __forceinline__ float dist_pairs_rounds(Load16 load, uint32_t units) {
+  float x0[2], y0[2], x1[2], y1[2], x2[2], y2[2], x3[2], y3[2];
+  level2_pair_rounds(load, 0, units, x0, y0);
+  level2_pair_rounds(load, 2, units, x2, y2);
+  level2_pair_rounds(load, 1, units, x1, y1);
+  level2_pair_rounds(load, 3, units, x3, y3);
+  add2(x0[0], y0[0], x2[0], y2[0]);
+  add2(x0[1], y0[1], x2[1], y2[1]);
+  add2(x1[0], y1[0], x3[0], y3[0]);
+  add2(x1[1], y1[1], x3[1], y3[1]);
+  add2(x0[0], y0[0], x1[0], y1[0]);
+  add2(x0[1], y0[1], x1[1], y1[1]);
+  add2(x0[0], y0[0], x0[1], y0[1]);
+  return __fadd_rn(x0[0], y0[0]);
+}
+
 __device__ __forceinline__ float row_dist128(const __half* __restrict__ a,
                                              const __half* __restrict__ b) {
   const uint4* A = reinterpret_cast<const uint4*>(a);
@@ -217,6 +260,11 @@ static __device__ __noinline__ float row_dist(const __half* __restrict__ a,
   const uint2* A = reinterpret_cast<const uint2*>(a);
   const uint2* B = reinterpret_cast<const uint2*>(b);
   if (dim == 128) return row_dist128(a, b);
+  if ((dim & 7u) == 0) {
+    const uint4* A4 = reinterpret_cast<const uint4*>(a);
+    const uint4* B4 = reinterpret_cast<const uint4*>(b);
+    return dist_pairs_rounds([&](uint32_t u, int w) { return __ldg((w ? B4 : A4) + u); }, dim >> 3);
+  }
   const uint32_t chunks = dim >> 2;
   auto leaf = [&](int slot, float& x, float& y) {
     for (uint32_t j = slot; j < chunks; j += 32) chunk_acc(__ldg(A + j), __ldg(B + j), x, y);

@@ -689,16 +689,27 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
       TG_CUDA(cudaMemcpyAsync(h2, w.stats + 5, sizeof(h2), cudaMemcpyDeviceToHost, s));
       TG_CUDA(cudaStreamSynchronize(s));
       sst.last_best_kept = h2[3] ? (double)h2[4] / (double)h2[3] : 0.0;
-      // miss rate of the screen on the sampled nodes steers the kept count;
-      // a screen that misses most improving pairs even at the largest count
-      // hands the remaining iterations to the exact join
+      // miss rate of the screen on the sampled nodes steers the kept count.
+      // A screen that misses most improving pairs (three in four at any
+      // count, or half at the largest) hands the join to the exact path: this
+      // iteration's join is run again exactly, its proposals joining the
+      // screened ones in the pool, so no iteration is lost to the screen.
       const double miss = h2[0] ? 1.0 - (double)h2[1] / (double)h2[0] : 0.0;
       sst.last_miss = miss;
       sst.screened_iters += 1;
       if (adapt) {
-        if (miss > 0.10 && lt < kLearnedMaxT) lt = std::min<uint32_t>(kLearnedMaxT, lt + 2);
-        else if (miss < 0.02 && lt > 2) lt -= 1;
-        if (miss > 0.5 && lt == kLearnedMaxT) fallback = true;
+        if (miss > 0.75 || (miss > 0.5 && lt == kLearnedMaxT)) {
+          fallback = true;
+          stage_begin(join_name, s);
+          if (!tc_supported(w.dim)) TG_TRY(join_plain(w, s));
+          else TG_TRY(join_tc(w, s));
+          count_launch();
+          stage_end(join_name, s);
+        } else if (miss > 0.10 && lt < kLearnedMaxT) {
+          lt = std::min<uint32_t>(kLearnedMaxT, lt + 2);
+        } else if (miss < 0.02 && lt > 2) {
+          lt -= 1;
+        }
       }
     } else {
       stage_begin(join_name, s);
