@@ -585,6 +585,14 @@ int join_plain(const Work& w, cudaStream_t s) {
 
 }  // namespace knn
 
+// The exact join for a width and mode: the tensor-core tile up to 128 dims,
+// the K-streamed tile up to 1024, otherwise (and in the plain mode) FP32 SIMT.
+static int join_exact(const knn::Work& w, uint32_t mode, cudaStream_t s) {
+  if (mode != TAGORE_KNN_PLAIN && knn::tc_supported(w.dim)) return knn::join_tc(w, s);
+  if (mode != TAGORE_KNN_PLAIN && knn::tc_wide_supported(w.dim)) return knn::join_tc_wide(w, s);
+  return knn::join_plain(w, s);
+}
+
 int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, cudaStream_t s) {
   using namespace knn;
   if (d.n < 2 || a.k == 0 || a.k >= d.n) return fail(TAGORE_EINVAL, "need POINTS > K >= 1");
@@ -634,12 +642,14 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   count_launch();
   stage_end("knn_init", s, n64 * K * (2ull * d.dim + 8), n64 * K);
   TG_CUDA(cudaGetLastError());
-  const char* join_name = a.mode == TAGORE_KNN_PLAIN ? "knn_join_plain" : "knn_join_tc";
-  // The learned screen serves the chosen path where the tensor-core tile does
-  // not apply (and every width when asked for): the first iterations run the
+  const bool tc_width = tc_supported(d.dim) || tc_wide_supported(d.dim);
+  const char* join_name = a.mode == TAGORE_KNN_PLAIN || !tc_width ? "knn_join_plain"
+                          : tc_supported(d.dim)                   ? "knn_join_tc"
+                                                                  : "knn_join_tc_wide";
+  // The learned screen serves the chosen path where no tensor-core tile
+  // applies (and every width when asked for): the first iterations run the
   // exact join, then the MLP is trained on their rows and screens the rest.
-  const bool learned = a.mode == TAGORE_KNN_LEARNED ||
-                       (a.mode == TAGORE_KNN_CHOSEN && !tc_supported(d.dim));
+  const bool learned = a.mode == TAGORE_KNN_LEARNED || (a.mode == TAGORE_KNN_CHOSEN && !tc_width);
   const uint32_t warm = std::min<uint32_t>(2, a.iters);
   uint32_t lt = a.per_row ? std::min<uint32_t>(std::max<uint32_t>(a.per_row, 2), kLearnedMaxT) : 4;
   const bool adapt = !(a.learn_flags & TAGORE_LEARN_FIXED_T);
@@ -701,8 +711,7 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
         if (miss > 0.75 || (miss > 0.5 && lt == kLearnedMaxT)) {
           fallback = true;
           stage_begin(join_name, s);
-          if (!tc_supported(w.dim)) TG_TRY(join_plain(w, s));
-          else TG_TRY(join_tc(w, s));
+          TG_TRY(join_exact(w, a.mode, s));
           count_launch();
           stage_end(join_name, s);
         } else if (miss > 0.10 && lt < kLearnedMaxT) {
@@ -713,11 +722,7 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
       }
     } else {
       stage_begin(join_name, s);
-      if (a.mode == TAGORE_KNN_PLAIN || !tc_supported(w.dim)) {
-        TG_TRY(join_plain(w, s));
-      } else {
-        TG_TRY(join_tc(w, s));
-      }
+      TG_TRY(join_exact(w, a.mode, s));
       count_launch();
       stage_end(join_name, s);
     }

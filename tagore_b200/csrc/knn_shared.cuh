@@ -30,6 +30,9 @@ struct Work {
 int join_tc(const Work& w, cudaStream_t s);
 // Row widths the tensor-core join takes (one 128-row tile of K-major FP16).
 inline bool tc_supported(uint32_t dim) { return dim >= 16 && dim <= 128 && dim % 16 == 0; }
+// Wider rows: the Gram tile accumulated over 64-half column blocks.
+int join_tc_wide(const Work& w, cudaStream_t s);
+inline bool tc_wide_supported(uint32_t dim) { return dim > 128 && dim <= 1024 && dim % 8 == 0; }
 
 __device__ __forceinline__ uint64_t make_key(float d, uint32_t id, bool is_new) {
   return ((uint64_t)__float_as_uint(d) << 32) | ((uint64_t)id << 1) | (is_new ? 1ull : 0ull);

@@ -493,6 +493,347 @@ __global__ void __launch_bounds__(kThreads, 3)
                  "r"(kTmemCols));
 }
 
+// ---------------------------------------------------------------------------
+// Wide rows (128 < d <= 1024). A 128-row FP16 tile no longer fits in shared
+// memory, so the Gram tile accumulates over K as a GEMM's K loop does: the
+// producer warp gathers one 64-half column block of the node's rows at a time
+// into a ring of stages, a dedicated MMA warp adds each block's four K = 16
+// steps into one of two TMEM accumulators and frees the stage when its MMAs
+// complete, and the four consumer warps screen the finished tile exactly as
+// k_join_tc does. The kept pairs are re-ranked from the base rows in global
+// memory (the tile's rows have left the ring by then). TMA fills past d with
+// zeros, which leave the Gram sums unchanged. The FP32 accumulation error of a
+// Gram entry over d <= 1024 terms stays below 1024 * 2^-24 * (n_r + n_c) / 2 =
+// 2^-15 (n_r + n_c), inside the screen's 2^-12 (n_r + n_c) margin.
+constexpr int kWideRing = 6;                       // column blocks in flight
+constexpr int kWideNodes = 2;                      // node metadata slots
+constexpr int kWideThreads = kConsumers + 64;      // consumers, producer (warp 4), MMA (warp 5)
+constexpr uint32_t kWideTmemCols = 256;            // two 128-column accumulators
+constexpr uint32_t kWideMaxDim = 1024;
+
+struct __align__(1024) WideSmem {
+  uint8_t ring[kWideRing][kMaxList][128];  // one column block: [row][128 B], SW128
+  uint32_t ids[kWideNodes][kMaxList];
+  float hnrm[kWideNodes][kMaxList];  // (1 - 2^-12) x exact squared norm
+  float kth[kWideNodes][kMaxList];
+  uint32_t pairs[kConsumers * 4];
+  uint32_t warp_pairs[kConsumers / 32];
+  unsigned long long ring_full[kWideRing], ring_empty[kWideRing];
+  unsigned long long node_full[kWideNodes], node_empty[kWideNodes];
+  unsigned long long acc_full[2], acc_empty[2], drain;
+  uint32_t taddr;
+  uint32_t node[kWideNodes], nn[kWideNodes], total[kWideNodes];
+  uint32_t filled, taken;  // column blocks the producer issued / the MMA warp waited for
+  int flag;
+};
+
+// Producer warp of the wide join: node metadata into slot j % 2, then the
+// node's column blocks, each into the next ring stage once the MMAs that read
+// it before have completed.
+__device__ void wide_producer(WideSmem& s, const CUtensorMap& tmap, const uint64_t* __restrict__ nb,
+                              const float* __restrict__ norms, const uint32_t* __restrict__ lists,
+                              const uint32_t* __restrict__ lcnt, uint32_t n, uint32_t dim,
+                              uint32_t K, unsigned long long* n_rows) {
+  const uint32_t lane = threadIdx.x & 31u, blocks = (dim + 63) / 64;
+  uint32_t next = blockIdx.x, fill = 0;
+  uint32_t ph_node[kWideNodes] = {};
+  for (uint32_t j = 0;; ++j) {
+    const int ns = (int)(j % kWideNodes);
+    if (j >= (uint32_t)kWideNodes) {
+      bool ok = true;
+      if (lane == 0) {
+        ok = mbar_wait_bounded(smem_u32(&s.node_empty[ns]), ph_node[ns]);
+        if (!ok) s.flag = 0;
+      }
+      ph_node[ns] ^= 1u;
+      if (!__shfl_sync(kFull, ok ? 1 : 0, 0)) return;
+    }
+    uint32_t u = kDone, nn = 0, tot = 0;
+    while (next < n) {
+      const uint32_t c = next + lane * gridDim.x;
+      uint2 cnt = make_uint2(0, 0);
+      if (c < n) cnt = *reinterpret_cast<const uint2*>(lcnt + 2 * (size_t)c);
+      const unsigned ok = __ballot_sync(kFull, c < n && cnt.x > 0 && cnt.y >= 2);
+      if (ok) {
+        const int w = __ffs(ok) - 1;
+        u = next + (uint32_t)w * gridDim.x;
+        nn = __shfl_sync(kFull, cnt.x, w);
+        tot = __shfl_sync(kFull, cnt.y, w);
+        next = u + gridDim.x;
+        break;
+      }
+      next += 32u * gridDim.x;
+    }
+    for (uint32_t t = lane; t < tot; t += 32) {
+      const uint32_t id = lists[(size_t)u * kMaxList + t];
+      s.ids[ns][t] = id;
+      s.hnrm[ns][t] = kOneMinusEps * norms[id];
+      s.kth[ns][t] = kth_of(nb[(size_t)id * K + K - 1]);
+    }
+    if (lane == 0) {
+      s.node[ns] = u;
+      s.nn[ns] = nn;
+      s.total[ns] = tot;
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_u32(&s.node_full[ns]));
+    if (u == kDone) return;
+    if (lane == 0) *n_rows += tot;
+    const uint32_t groups = (tot + 3) / 4;
+    for (uint32_t b = 0; b < blocks; ++b, ++fill) {
+      const int slot = (int)(fill % kWideRing);
+      const uint32_t bar = smem_u32(&s.ring_full[slot]);
+      bool ok = true;
+      if (lane == 0) {
+        if (fill >= (uint32_t)kWideRing)
+          ok = mbar_wait_bounded(smem_u32(&s.ring_empty[slot]), ((fill / kWideRing) - 1) & 1u);
+        if (!ok) {
+          s.flag = 0;
+        } else {
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                       "r"(groups * 4 * 128)
+                       : "memory");
+          s.filled = fill + 1;
+        }
+      }
+      if (!__shfl_sync(kFull, ok ? 1 : 0, 0)) return;
+      for (uint32_t g = lane; g < groups; g += 32) {
+        uint32_t r[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) r[t] = s.ids[ns][min(4 * g + t, tot - 1)];
+        const uint32_t dst = smem_u32(&s.ring[slot][4 * g][0]);
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::"
+            "bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dst),
+            "l"(reinterpret_cast<uint64_t>(&tmap)), "r"(b * 64), "r"(r[0]), "r"(r[1]), "r"(r[2]),
+            "r"(r[3]), "r"(bar)
+            : "memory");
+      }
+    }
+  }
+}
+
+// MMA thread of the wide join: node j's Gram tile into accumulator j % 2,
+// one column block (four K = 16 steps) at a time.
+__device__ void wide_mma(WideSmem& s, uint32_t tmem, uint32_t dim) {
+  const uint32_t blocks = (dim + 63) / 64;
+  uint32_t ph_node[kWideNodes] = {}, ph_acc[2] = {}, take = 0;
+  for (uint32_t j = 0;; ++j) {
+    const int ns = (int)(j % kWideNodes), acc = (int)(j % 2);
+    if (!mbar_wait_bounded(smem_u32(&s.node_full[ns]), ph_node[ns])) {
+      s.flag = 0;
+      break;
+    }
+    ph_node[ns] ^= 1u;
+    if (s.node[ns] == kDone) {
+      mbar_arrive(smem_u32(&s.acc_full[acc]));  // wakes the consumers, who see kDone
+      break;
+    }
+    if (j >= 2) {
+      if (!mbar_wait_bounded(smem_u32(&s.acc_empty[acc]), ph_acc[acc])) {
+        s.flag = 0;
+        break;
+      }
+      ph_acc[acc] ^= 1u;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    bool ok = true;
+    for (uint32_t b = 0; b < blocks && ok; ++b, ++take) {
+      const int slot = (int)(take % kWideRing);
+      ok = mbar_wait_bounded(smem_u32(&s.ring_full[slot]), (take / kWideRing) & 1u);
+      if (!ok) break;
+      s.taken = take + 1;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) {
+        const uint64_t desc = sw128_desc(smem_u32(&s.ring[slot][0][0]) + k * 32);
+        const uint32_t accum = (b | k) != 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem + acc * 128),
+            "l"(desc), "l"(desc), "r"(kIdesc), "r"(accum));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(&s.ring_empty[slot])));
+    }
+    if (!ok) {
+      s.flag = 0;
+      break;
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+        smem_u32(&s.acc_full[acc])));
+  }
+  // every MMA this thread issued has completed before TMEM is released
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+      smem_u32(&s.drain)));
+  if (!mbar_wait_bounded(smem_u32(&s.drain), 0)) s.flag = 0;
+}
+
+__global__ void __launch_bounds__(kWideThreads, 2)
+    k_join_tc_wide(const __grid_constant__ CUtensorMap tmap, const __half* __restrict__ data,
+                   const uint64_t* __restrict__ nb, const float* __restrict__ norms,
+                   const uint32_t* __restrict__ lists, const uint32_t* __restrict__ lcnt,
+                   uint32_t n, uint32_t dim, uint32_t K, uint32_t T, uint32_t P,
+                   unsigned long long* __restrict__ pool, unsigned long long* __restrict__ stats,
+                   int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  WideSmem& s = *reinterpret_cast<WideSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t tid = threadIdx.x, warp = tid >> 5;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s.taddr)),
+                 "r"(kWideTmemCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < kWideRing; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.ring_full[i])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.ring_empty[i])));
+    }
+    for (int i = 0; i < kWideNodes; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.node_full[i])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&s.node_empty[i])));
+    }
+    for (int i = 0; i < 2; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.acc_full[i])));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&s.acc_empty[i])));
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.drain)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    asm volatile("fence.proxy.async.shared::cta;");
+    s.flag = 1;
+    s.filled = 0;
+    s.taken = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = s.taddr;
+  unsigned long long n_pairs = 0, n_props = 0, n_rows = 0;
+
+  if (warp == 4) {
+    wide_producer(s, tmap, nb, norms, lists, lcnt, n, dim, K, &n_rows);
+  } else if (warp == 5) {
+    if ((tid & 31u) == 0) wide_mma(s, tmem, dim);
+    __syncwarp();
+  } else {
+    uint32_t ph_node[kWideNodes] = {}, ph_acc[2] = {};
+    const uint32_t r = tid, lane = tid & 31u;
+    for (uint32_t i = 0;; ++i) {
+      const int ns = (int)(i % kWideNodes), acc = (int)(i % 2);
+      bool ok = mbar_wait_bounded(smem_u32(&s.node_full[ns]), ph_node[ns]);
+      ph_node[ns] ^= 1u;
+      if (ok) ok = mbar_wait_bounded(smem_u32(&s.acc_full[acc]), ph_acc[acc]);
+      ph_acc[acc] ^= 1u;
+      // every consumer leaves together: on any thread's timeout, or at kDone
+      if (consumers_any(!ok)) {
+        if (tid == 0) s.flag = 0;
+        break;
+      }
+      if (s.node[ns] == kDone) break;
+      const uint32_t nn = s.nn[ns], total = s.total[ns];
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      // ---- screen: the same rule and order as k_join_tc ----
+      const bool live = r < total;
+      const float lim = live ? s.kth[ns][r] - s.hnrm[ns][r] : -INFINITY;
+      float bd[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+      uint32_t bc[4] = {kInv, kInv, kInv, kInv};
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if ((uint32_t)t >= T) bd[t] = -INFINITY;
+      const uint32_t cmax = live ? ((r < nn) ? total : nn) : 0u;
+      const uint32_t wmax = __reduce_max_sync(kFull, cmax);
+      float cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
+#pragma unroll 1
+      for (uint32_t q = 0; q * 32 < wmax; ++q) {
+        float g[32];
+        tmem_ld32(tmem + acc * 128 + ((warp * 32u) << 16) + q * 32u, g);
+        if (q * 32 >= cmax) continue;
+        const float4* h4 = reinterpret_cast<const float4*>(&s.hnrm[ns][q * 32]);
+#pragma unroll
+        for (int k4 = 0; k4 < 8; ++k4) {
+          const float4 h = h4[k4];
+          float v4[4];
+          fma2_m2(g[4 * k4], g[4 * k4 + 1], h.x, h.y, v4[0], v4[1]);
+          fma2_m2(g[4 * k4 + 2], g[4 * k4 + 3], h.z, h.w, v4[2], v4[3]);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const uint32_t c = q * 32 + 4 * k4 + j;
+            if (v4[j] < cut && c < cmax && c != r) {
+              float v = v4[j];
+              uint32_t vc = c;
+#pragma unroll
+              for (int t = 0; t < 4; ++t)
+                if (v < bd[t]) {
+                  swap_(v, bd[t]);
+                  swap_(vc, bc[t]);
+                }
+              cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
+            }
+          }
+        }
+      }
+      // the accumulator is read: the MMA warp may refill it with node i + 2
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&s.acc_empty[acc]));
+      uint32_t kept = 0;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) kept += bc[t] != kInv ? 1u : 0u;
+      uint32_t incl = kept;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+      }
+      if (lane == 31) s.warp_pairs[warp] = incl;
+      consumers_sync();
+      uint32_t off = incl - kept, npairs = 0;
+#pragma unroll
+      for (int w = 0; w < kConsumers / 32; ++w) {
+        const uint32_t c = s.warp_pairs[w];
+        if ((uint32_t)w < warp) off += c;
+        npairs += c;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t)
+        if (bc[t] != kInv) s.pairs[off++] = (r << 16) | bc[t];
+      consumers_sync();
+      // ---- exact re-rank of the kept pairs from the base rows ----
+      for (uint32_t q = tid; q < npairs; q += kConsumers) {
+        const uint32_t pr = s.pairs[q], row = pr >> 16, col = pr & 0xFFFFu;
+        const uint32_t a = s.ids[ns][row], c = s.ids[ns][col];
+        const float d = row_dist(data + (size_t)a * dim, data + (size_t)c * dim, dim);
+        ++n_pairs;
+        if (d < s.kth[ns][row]) {
+          propose(pool, a, P, c, d);
+          ++n_props;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&s.node_empty[ns]));
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && !s.flag) {
+    // after a timeout, column blocks the MMA thread never waited for land
+    // before the block's shared memory is released
+    for (uint32_t f = s.taken; f < s.filled; ++f)
+      mbar_wait_bounded(smem_u32(&s.ring_full[f % kWideRing]), (f / kWideRing) & 1u);
+  }
+  __syncthreads();
+  if (!s.flag && tid == 0) atomicExch(err, 1);
+  if (n_props) atomicAdd(&stats[0], n_props);
+  if (n_pairs) atomicAdd(&stats[1], n_pairs);
+  if (n_rows) atomicAdd(&stats[3], n_rows);
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kWideTmemCols));
+}
+
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -536,7 +877,31 @@ int launch(const Work& w, const CUtensorMap& map, cudaStream_t s) {
   return TAGORE_OK;
 }
 
+int launch_wide(const Work& w, const CUtensorMap& map, cudaStream_t s) {
+  const size_t sm = sizeof(WideSmem) + 1024;
+  TG_CUDA(cudaFuncSetAttribute((const void*)k_join_tc_wide,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int* err = reinterpret_cast<int*>(w.stats + 4);
+  k_join_tc_wide<<<sms * 2, kWideThreads, sm, s>>>(map, w.data, w.nb, w.norms, w.lists, w.lcnt,
+                                                    w.n, w.dim, w.K, w.T, w.P, w.pool, w.stats, err);
+  TG_CUDA(cudaGetLastError());
+  return TAGORE_OK;
+}
+
 }  // namespace
+
+int join_tc_wide(const Work& w, cudaStream_t s) {
+  if (!tc_wide_supported(w.dim))
+    return fail(TAGORE_EINVAL, "wide tensor-core join needs 128 < DIM <= 1024, DIM %% 8 == 0 (got %u)",
+                w.dim);
+  if (w.T > 4) return fail(TAGORE_EINVAL, "tensor-core join keeps at most 4 partners per row");
+  CUtensorMap map;
+  TG_TRY(make_row_map(&map, w.data, w.n, w.dim));
+  return launch_wide(w, map, s);
+}
 
 int join_tc(const Work& w, cudaStream_t s) {
   if (w.dim > 128 || w.dim % 16)

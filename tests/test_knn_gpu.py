@@ -49,11 +49,14 @@ def test_knn_recall(capi, orc, mode):
     assert r > 0.95, r
 
 
-@pytest.mark.parametrize("kind,dim", [("deep", 96), ("gist", 960), ("sift", 200)])
+@pytest.mark.parametrize("kind,dim", [("deep", 96), ("gist", 960), ("sift", 200), ("deep", 136),
+                                      ("gist", 1024)])
 @pytest.mark.parametrize("mode", ["plain", "chosen"])
 def test_knn_other_widths(capi, orc, kind, dim, mode):
-    """Row widths beside 128: 96 (tensor-core screen), 960 and 200 (rows read
-    from the cache hierarchy; the chosen mode falls back to the plain join)."""
+    """Row widths beside 128: 96 (one tensor-core tile) and, above 128, the
+    K-streamed tensor-core join in the chosen mode: 960, 200, 136 (a last
+    column block mostly zero-filled) and 1024 (sixteen full blocks); the plain
+    mode reads rows from the cache hierarchy."""
     base, _ = synth.mixture(kind, 4000, dim, 16, 23)
     K = 32
     g, d, half = build(capi, base, K, 8, capi.KNN_PLAIN if mode == "plain" else capi.KNN_CHOSEN)

@@ -55,12 +55,18 @@ def build(capi, base, K, iters, mode, **kw):
     return g, d, half, capi.last_screen()
 
 
-def test_chosen_path_at_960_uses_the_trained_screen(capi, orc):
+def test_learned_path_at_960_trains_and_screens(capi, orc):
+    """The learned mode at d = 960 trains the screen, screens at least one
+    iteration (handing over to the exact join where it misses too much) and
+    stores only exact distances. The chosen mode at this width is the
+    K-streamed tensor-core join, which uses no screen."""
     base, _ = synth.mixture("gist", 6000, 960, 32, 41)
     K = 32
-    g, d, half, scr = build(capi, base, K, 8, capi.KNN_CHOSEN)
+    g, d, half, scr = build(capi, base, K, 8, capi.KNN_LEARNED)
     n = base.shape[0]
     assert scr.used == 1 and scr.steps == 400 and scr.screened_iters >= 1
+    _, _, _, chosen = build(capi, base, K, 4, capi.KNN_CHOSEN)
+    assert chosen.used == 0
     assert scr.loss_last < scr.loss_first
     # every stored distance is exact
     exp = orc.dist_pairs(half, np.repeat(np.arange(n), K), g.reshape(-1)).reshape(n, K)
