@@ -801,14 +801,43 @@ __global__ void __launch_bounds__(kWideThreads, 2)
         if (bc[t] != kInv) s.pairs[off++] = (r << 16) | bc[t];
       consumers_sync();
       // ---- exact re-rank of the kept pairs from the base rows ----
-      for (uint32_t q = tid; q < npairs; q += kConsumers) {
-        const uint32_t pr = s.pairs[q], row = pr >> 16, col = pr & 0xFFFFu;
-        const uint32_t a = s.ids[ns][row], c = s.ids[ns][col];
-        const float d = row_dist(data + (size_t)a * dim, data + (size_t)c * dim, dim);
-        ++n_pairs;
-        if (d < s.kth[ns][row]) {
-          propose(pool, a, P, c, d);
-          ++n_props;
+      // Four lanes per pair, one level-2 quarter p of the reference tree each
+      // (dist_pairs_rounds), combined in that function's order: p += p + 2,
+      // then p0 += p1, then x + y. Each lane walks a quarter of the loads.
+      const uint32_t sub = lane & 3u;
+      for (uint32_t base = 0; base < npairs; base += kConsumers / 4) {
+        const uint32_t q = base + (tid >> 2);
+        const bool have = q < npairs;
+        float x[2] = {0.0f, 0.0f}, y[2] = {0.0f, 0.0f};
+        uint32_t row = 0, a = 0, c = 0;
+        if (have) {
+          const uint32_t pr = s.pairs[q];
+          row = pr >> 16;
+          a = s.ids[ns][row];
+          c = s.ids[ns][pr & 0xFFFFu];
+          const uint4* A4 = reinterpret_cast<const uint4*>(data + (size_t)a * dim);
+          const uint4* B4 = reinterpret_cast<const uint4*>(data + (size_t)c * dim);
+          auto load = [&](uint32_t u, int w) { return __ldg((w ? B4 : A4) + u); };
+          level2_pair_rounds(load, (int)sub, dim >> 3, x, y);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float ox = __shfl_xor_sync(kFull, x[h], 2), oy = __shfl_xor_sync(kFull, y[h], 2);
+          if (sub < 2) add2(x[h], y[h], ox, oy);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float ox = __shfl_xor_sync(kFull, x[h], 1), oy = __shfl_xor_sync(kFull, y[h], 1);
+          if (sub == 0) add2(x[h], y[h], ox, oy);
+        }
+        if (have && sub == 0) {
+          add2(x[0], y[0], x[1], y[1]);
+          const float d = __fadd_rn(x[0], y[0]);
+          ++n_pairs;
+          if (d < s.kth[ns][row]) {
+            propose(pool, a, P, c, d);
+            ++n_props;
+          }
         }
       }
       __syncwarp();
