@@ -82,3 +82,62 @@ def test_large_index_single_device(capi, orc, tmp_path):
     truth = np.argsort(d2, 1)[:, :10]
     rec = np.mean([len(set(a) & set(b)) / 10 for a, b in zip(found.tolist(), truth.tolist())])
     assert rec > 0.8, rec
+
+
+def test_large_index_uneven_clusters_recall_and_rate(capi, tmp_path):
+    """The configuration's shape at a smaller scale: 24 clusters of lognormal
+    sizes, unit-normalised d = 96 points each stored in its two nearest of 24
+    centres, k = 64, max_degree 22, alpha 1.2. The merged file is read back
+    with the Vamana reader (the same layout), searched on the GPU from its
+    medoid, and scored by recall@10 against brute force on 2,000 held-out
+    queries; the build rate is printed."""
+    import time
+
+    import torch
+    rng = np.random.default_rng(5)
+    cn, dim = 24, 96
+    sizes = np.clip(np.exp(rng.normal(np.log(25000), 0.8, cn)), 5000, 120000).astype(int)
+    n = int(sizes.sum()) // 2
+    centers = rng.normal(0, 1, size=(cn, dim)).astype(np.float32)
+
+    def draw(m):
+        y = centers[rng.integers(0, cn, m)] + rng.normal(0, 0.35, size=(m, dim)).astype(np.float32)
+        return (y / np.linalg.norm(y, axis=1, keepdims=True)).astype(np.float32)
+
+    x, queries = draw(n), draw(2000)
+    order = np.argsort(-(x @ centers.T), 1)
+    first, second = order[:, 0].astype(np.uint32), order[:, 1].astype(np.uint32)
+    np.stack([first, second], 1).astype(np.uint32).tofile(tmp_path / "centers.bin")
+    members = [np.sort(np.concatenate([np.nonzero(first == c)[0], np.nonzero(second == c)[0]]))
+               for c in range(cn)]
+    for c in range(cn):
+        with open(tmp_path / f"cluster_{c}", "wb") as f:
+            f.write(struct.pack("<I", len(members[c])))
+            f.write(np.ascontiguousarray(x[members[c]]).tobytes())
+    out = tmp_path / "final.index"
+    p = params(capi, tmp_path, dim, 64, cn, max(len(m) for m in members), 22, 8, 32, 64, 1.2, 0,
+               out)
+    p.num = n
+    dev = (C.c_uint32 * 1)(0)
+    t = time.perf_counter()
+    capi.check(capi.lib().tagore_large_index(C.byref(p), dev, 1))
+    el = time.perf_counter() - t
+    builds = sum(len(m) for m in members)
+
+    info, offs, adj = capi.index_read(out, "Vamana")
+    assert info.n == n and info.max_degree <= 22 and info.eps[0] < n
+    cuda = torch.device("cuda:0")
+    xb = torch.as_tensor(x, device=cuda)
+    xq = torch.as_tensor(queries, device=cuda)
+    found = capi.search(xb, torch.as_tensor(offs.astype(np.int64), device=cuda),
+                        torch.as_tensor(adj.view(np.int32), device=cuda), info.eps[0], xq, 128,
+                        10, 0x5EED).cpu().numpy()
+    d2 = (xq * xq).sum(1, keepdim=True) + (xb * xb).sum(1)[None] - 2.0 * (xq @ xb.T)
+    truth = torch.topk(d2, 10, largest=False).indices.cpu().numpy()
+    recall = float(np.mean([len(set(a.tolist()) & set(b.tolist())) / 10
+                            for a, b in zip(found, truth)]))
+    print(f"largeIndex: {cn} clusters ({min(len(m) for m in members)}-{max(len(m) for m in members)}"
+          f" points), {n} points, {builds} point-builds in {el:.2f} s "
+          f"({builds / el / 1e6:.2f} M/s); recall@10 {recall:.4f}")
+    # measured 0.82 at pool size 128 (rows truncated to 22 neighbours by the merge)
+    assert recall > 0.75
