@@ -25,8 +25,10 @@ enum {
 };
 
 /* kNN join modes. CHOSEN: tensor-core screen + exact re-rank where the row
- * width allows (16..128 dims in steps of 16), the learned screen otherwise;
- * PLAIN: every pair in exact FP32; LEARNED: the learned screen at any width. */
+ * width allows (one tile for 16..128 dims in steps of 16; the tile
+ * accumulated over 64-dim blocks for 129..1024 dims in steps of 8), the
+ * learned screen otherwise; PLAIN: every pair in exact FP32; LEARNED: the
+ * learned screen at any width. */
 enum { TAGORE_KNN_CHOSEN = 0, TAGORE_KNN_PLAIN = 1, TAGORE_KNN_LEARNED = 2 };
 
 /* learn_flags of TagoreKnnParams (for measuring the screen against itself):
@@ -127,7 +129,9 @@ int tagore_pruning_cfs_noalloc(const TagorePruneParams* p, TagoreKnnState* st, c
                                const char* metric, void* stream);
 
 /* Tagore.largeIndex(devicelist, DIM, K, cluster_num, max_points, ...)
- * (pybind.cu:298-391) for a single device (devicelist = [0]). */
+ * (pybind.cu:298-391). One builder thread per devicelist entry (1 to 64; an id
+ * may repeat, which runs that many builders on one device) takes the clusters
+ * in the merger's order; the reference deals them round-robin. */
 int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev);
 
 /* The host half of largeIndex alone (reorder + order_merge_new,

@@ -611,7 +611,7 @@ int tagore_build_index_host(const TagoreKnnParams* p, const float* data, uint32_
 int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_rows,
                        const uint32_t* local_medoids) {
   if (!p || !local_rows || !local_medoids) return fail(TAGORE_EINVAL, "null argument");
-  LargeBuildFn given = [&](const TagoreLargeParams& q, uint32_t cid, const std::vector<uint32_t>& ids,
+  LargeBuildFn given = [&](const TagoreLargeParams& q, uint32_t, uint32_t cid, const std::vector<uint32_t>& ids,
                            std::vector<uint32_t>& rows, uint32_t* medoid) -> int {
     if (!local_rows[cid]) return fail(TAGORE_EINVAL, "no local graph for cluster %u", cid);
     rows.assign(local_rows[cid], local_rows[cid] + ids.size() * (size_t)q.k);
@@ -624,13 +624,13 @@ int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_
 
 int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev) {
   if (!p || !devices) return fail(TAGORE_EINVAL, "null argument");
-  const int device = (int)devices[0];
   // gpu_construct (src/large_index.cu:130-279) for one cluster: read
   // [u32 n][n x dim f32], kNN graph without rescale, CFS path/dist prune with
   // alpha = thre, rows back to the host with local ids mapped to global ones.
-  LargeBuildFn build = [device](const TagoreLargeParams& q, uint32_t cid, const std::vector<uint32_t>& ids,
-                                std::vector<uint32_t>& rows, uint32_t* medoid) -> int {
-    TG_CUDA(cudaSetDevice(device));
+  LargeBuildFn build = [devices](const TagoreLargeParams& q, uint32_t worker, uint32_t cid,
+                                 const std::vector<uint32_t>& ids, std::vector<uint32_t>& rows,
+                                 uint32_t* medoid) -> int {
+    TG_CUDA(cudaSetDevice((int)devices[worker]));
     const uint32_t n = (uint32_t)ids.size(), dim = q.dim;
     const std::string path = std::string(q.data_prefix) + std::to_string(cid);
     FILE* f = std::fopen(path.c_str(), "rb");

@@ -143,10 +143,13 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
 
 // ---- largeIndex (large_index.cpp) ----
 // Builds cluster `cid` (global ids `ids`) into n x K rows [deg, global ids..]
-// and reports its entry point as a global id.
-using LargeBuildFn = std::function<int(const TagoreLargeParams&, uint32_t cid,
+// and reports its entry point as a global id. `worker` is the builder thread,
+// an index into the device list.
+using LargeBuildFn = std::function<int(const TagoreLargeParams&, uint32_t worker, uint32_t cid,
                                        const std::vector<uint32_t>& ids,
                                        std::vector<uint32_t>& rows, uint32_t* medoid)>;
+// One builder thread per device-list entry, each taking the next cluster in
+// the merger's order; the host merger consumes them in that order.
 int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int ndev,
                     const LargeBuildFn& build);
 

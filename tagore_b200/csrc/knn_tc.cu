@@ -869,15 +869,16 @@ using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, 
                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 int make_row_map(CUtensorMap* map, const __half* base, uint32_t n, uint32_t dim) {
-  static EncodeTiled fn = nullptr;
-  if (!fn) {
+  // looked up once; a function-local static is initialised once across threads
+  static const EncodeTiled fn = []() -> EncodeTiled {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
-    TG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
-    if (!p || q != cudaDriverEntryPointSuccess)
-      return fail(TAGORE_ECUDA, "cuTensorMapEncodeTiled is unavailable");
-    fn = reinterpret_cast<EncodeTiled>(p);
-  }
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        !p || q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  if (!fn) return fail(TAGORE_ECUDA, "cuTensorMapEncodeTiled is unavailable");
   const cuuint64_t gdim[2] = {dim, n};
   const cuuint64_t gstride[1] = {(cuuint64_t)dim * 2};
   const cuuint32_t box[2] = {64, 1};

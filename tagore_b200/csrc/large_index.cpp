@@ -1,4 +1,4 @@
-// large_index.cpp -- single-device largeIndex (pybind.cu:298-391,
+// large_index.cpp -- largeIndex (pybind.cu:298-391,
 // src/large_index.cu): every point sits in two clusters; each cluster's local
 // graph is built on the GPU (kNN graph without rescale, CFS path prune with
 // alpha = thre), remapped to global ids and handed to a host merger that keeps
@@ -6,9 +6,12 @@
 // both are resident, spills evicted local graphs to local_prefix + cid, and
 // finally streams the DiskANN-style index.
 //
-// The builder (this thread, the GPU) runs ahead of the merger (a host thread)
-// through a bounded queue; every wait between them is bounded and ends in
-// TAGORE_ETIMEOUT. The merged bytes equal a sequential run of the reference's
+// One builder thread per entry of the device list takes the clusters in the
+// merger's order from a shared counter, so uneven clusters balance over the
+// devices as they come (the reference deals them round-robin,
+// src/large_index.cu:175); the builders run at most two clusters per device
+// ahead of the merger (a host thread). Every wait between them is bounded and
+// ends in TAGORE_ETIMEOUT. The merged bytes equal a sequential run of the reference's
 // merger (order_merge_new, :286-522) over the same local graphs.
 #include <algorithm>
 #include <chrono>
@@ -301,9 +304,8 @@ int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int nd
                     const LargeBuildFn& build) {
   if (!p.data_prefix || !p.local_prefix || !p.index_store_path || !p.centers_path)
     return fail(TAGORE_EINVAL, "largeIndex: null path");
-  if (ndev != 1)
-    return fail(TAGORE_EINVAL, "largeIndex runs on one device here (devicelist must hold one id)");
-  (void)dev_list;
+  if (ndev < 1 || ndev > 64 || !dev_list)
+    return fail(TAGORE_EINVAL, "largeIndex: devicelist must hold 1 to 64 device ids");
   const uint32_t C = p.cluster_num, N = p.num;
   if (C == 0 || N == 0 || p.buffer_size == 0 || p.k == 0 || p.max_degree == 0 || p.max_degree >= p.k)
     return fail(TAGORE_EINVAL, "largeIndex: need clusters, points, buffer_size > 0 and max_degree < K");
@@ -355,34 +357,55 @@ int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int nd
     if (merge_rc != TAGORE_OK && !sh.error) sh.error = merge_rc;
     sh.cv.notify_all();
   });
-  const uint32_t ahead = 2;  // clusters built but not yet merged
-  int rc = TAGORE_OK;
-  for (uint32_t i = 0; i < C && rc == TAGORE_OK; ++i) {
-    {
-      std::unique_lock<std::mutex> lk(sh.mu);
-      if (!wait_for(sh, lk, [&] { return sh.consumed + ahead > i; })) {
-        rc = fail(TAGORE_ETIMEOUT, "largeIndex: merger stalled");
-        break;
+  const uint32_t workers = (uint32_t)ndev;
+  const uint32_t ahead = 2 * workers;  // clusters built but not yet merged
+  uint32_t next = 0;                   // next cluster (merge order) to hand out, under sh.mu
+  auto builder = [&](uint32_t w) {
+    while (true) {
+      uint32_t i;
+      {
+        std::unique_lock<std::mutex> lk(sh.mu);
+        if (!wait_for(sh, lk, [&] { return next >= C || sh.consumed + ahead > next; })) {
+          if (!sh.error) {
+            sh.error = TAGORE_ETIMEOUT;
+            sh.msg = "largeIndex: merger stalled";
+          }
+          sh.cv.notify_all();
+          return;
+        }
+        if (sh.error || next >= C) return;
+        i = next++;
       }
-      if (sh.error) break;
+      const uint32_t cid = order[i];
+      std::vector<uint32_t> rows;
+      uint32_t medoid = 0;
+      const int rc = build(q, w, cid, clusters[cid], rows, &medoid);
+      std::lock_guard<std::mutex> g(sh.mu);
+      if (rc != TAGORE_OK) {
+        if (!sh.error) {
+          sh.error = rc;
+          sh.msg = tagore_last_error();
+        }
+      } else {
+        sh.built[i].rows.swap(rows);
+        sh.built[i].medoid = medoid;
+        sh.built[i].ready = true;
+      }
+      sh.cv.notify_all();
+      if (rc != TAGORE_OK) return;
     }
-    const uint32_t cid = order[i];
-    std::vector<uint32_t> rows;
-    uint32_t medoid = 0;
-    rc = build(q, cid, clusters[cid], rows, &medoid);
-    std::lock_guard<std::mutex> g(sh.mu);
-    if (rc != TAGORE_OK) {
-      sh.error = rc;
-      sh.msg = tagore_last_error();
-    } else {
-      sh.built[i].rows.swap(rows);
-      sh.built[i].medoid = medoid;
-      sh.built[i].ready = true;
-    }
-    sh.cv.notify_all();
-  }
+  };
+  std::vector<std::thread> pool;
+  for (uint32_t w = 1; w < workers; ++w) pool.emplace_back(builder, w);
+  builder(0);  // the calling thread is builder 0
+  for (auto& t : pool) t.join();
   merger.join();
-  if (rc != TAGORE_OK) return fail(rc, "%s", sh.msg.empty() ? tagore_last_error() : sh.msg.c_str());
+  int rc;
+  {
+    std::lock_guard<std::mutex> g(sh.mu);
+    rc = merge_rc == TAGORE_OK ? sh.error : TAGORE_OK;
+  }
+  if (rc != TAGORE_OK) return fail(rc, "%s", sh.msg.c_str());
   if (merge_rc != TAGORE_OK) return fail(merge_rc, "%s", merge_msg.c_str());
   return TAGORE_OK;
 }

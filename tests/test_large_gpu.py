@@ -114,30 +114,33 @@ def test_large_index_uneven_clusters_recall_and_rate(capi, tmp_path):
         with open(tmp_path / f"cluster_{c}", "wb") as f:
             f.write(struct.pack("<I", len(members[c])))
             f.write(np.ascontiguousarray(x[members[c]]).tobytes())
-    out = tmp_path / "final.index"
-    p = params(capi, tmp_path, dim, 64, cn, max(len(m) for m in members), 22, 8, 32, 64, 1.2, 0,
-               out)
-    p.num = n
-    dev = (C.c_uint32 * 1)(0)
-    t = time.perf_counter()
-    capi.check(capi.lib().tagore_large_index(C.byref(p), dev, 1))
-    el = time.perf_counter() - t
     builds = sum(len(m) for m in members)
-
-    info, offs, adj = capi.index_read(out, "Vamana")
-    assert info.n == n and info.max_degree <= 22 and info.eps[0] < n
+    capi.gnn_descent_host(x[:max(len(m) for m in members)], 64, 2).free()  # pool warm-up
     cuda = torch.device("cuda:0")
     xb = torch.as_tensor(x, device=cuda)
     xq = torch.as_tensor(queries, device=cuda)
-    found = capi.search(xb, torch.as_tensor(offs.astype(np.int64), device=cuda),
-                        torch.as_tensor(adj.view(np.int32), device=cuda), info.eps[0], xq, 128,
-                        10, 0x5EED).cpu().numpy()
     d2 = (xq * xq).sum(1, keepdim=True) + (xb * xb).sum(1)[None] - 2.0 * (xq @ xb.T)
     truth = torch.topk(d2, 10, largest=False).indices.cpu().numpy()
-    recall = float(np.mean([len(set(a.tolist()) & set(b.tolist())) / 10
-                            for a, b in zip(found, truth)]))
-    print(f"largeIndex: {cn} clusters ({min(len(m) for m in members)}-{max(len(m) for m in members)}"
-          f" points), {n} points, {builds} point-builds in {el:.2f} s "
-          f"({builds / el / 1e6:.2f} M/s); recall@10 {recall:.4f}")
-    # measured 0.82 at pool size 128 (rows truncated to 22 neighbours by the merge)
-    assert recall > 0.75
+    # devicelist [0]: one builder; [0, 0]: two builder threads sharing the GPU
+    # (their kernels never wait on each other), as several devices would
+    for devs in ([0], [0, 0]):
+        out = tmp_path / f"final_{len(devs)}.index"
+        p = params(capi, tmp_path, dim, 64, cn, max(len(m) for m in members), 22, 8, 32, 64, 1.2,
+                   0, out)
+        p.num = n
+        dev = (C.c_uint32 * len(devs))(*devs)
+        t = time.perf_counter()
+        capi.check(capi.lib().tagore_large_index(C.byref(p), dev, len(devs)))
+        el = time.perf_counter() - t
+        info, offs, adj = capi.index_read(out, "Vamana")
+        assert info.n == n and info.max_degree <= 22 and info.eps[0] < n
+        found = capi.search(xb, torch.as_tensor(offs.astype(np.int64), device=cuda),
+                            torch.as_tensor(adj.view(np.int32), device=cuda), info.eps[0], xq, 128,
+                            10, 0x5EED).cpu().numpy()
+        recall = float(np.mean([len(set(a.tolist()) & set(b.tolist())) / 10
+                                for a, b in zip(found, truth)]))
+        print(f"largeIndex devicelist {devs}: {cn} clusters ({min(len(m) for m in members)}-"
+              f"{max(len(m) for m in members)} points), {n} points, {builds} point-builds in "
+              f"{el:.2f} s ({builds / el / 1e6:.2f} M/s); recall@10 {recall:.4f}")
+        # measured 0.82 at pool size 128 (rows truncated to 22 neighbours by the merge)
+        assert recall > 0.75
