@@ -139,7 +139,9 @@ int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int 
  * p->centers_path as in tagore_large_index, but each cluster's local graph is
  * given: local_rows[cid] holds clusters[cid].size() x p->k rows of
  * [degree, global ids...] and local_medoids[cid] its entry point (a global
- * id). Writes the spill files and p->index_store_path; no device is used. */
+ * id). Writes the spill files and p->index_store_path; no device is used.
+ * Four builder threads hand the graphs over, as in a multi-device run; the
+ * merged bytes do not depend on their schedule. */
 int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_rows,
                        const uint32_t* local_medoids);
 

@@ -618,8 +618,10 @@ int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_
     *medoid = local_medoids[cid];
     return TAGORE_OK;
   };
-  const uint32_t dev0 = 0;
-  return large_index_run(*p, &dev0, 1, given);
+  // Four builder threads hand the given graphs to the merger: the schedule of
+  // a multi-device run, whose merged bytes must not depend on it.
+  const uint32_t workers[4] = {0, 0, 0, 0};
+  return large_index_run(*p, workers, 4, given);
 }
 
 int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev) {
