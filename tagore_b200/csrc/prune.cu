@@ -51,8 +51,8 @@ struct Beam {
   uint8_t* sex;    // staging (W + 1): their explored flags
 };
 
-// Hash slots: a power of two holding the beam at load <= 3/4 (TOPM <= 256, K <= 128).
-__host__ __device__ inline uint32_t hash_slots(uint32_t W) { return W <= 192 ? 256u : 512u; }
+// Hash slots: a power of two holding the beam at load <= 3/8 (TOPM <= 256, K <= 128).
+__host__ __device__ inline uint32_t hash_slots(uint32_t W) { return W <= 192 ? 512u : 1024u; }
 
 __host__ __device__ inline size_t beam_bytes(uint32_t W) {
   return (size_t)hash_slots(W) * 4 + (size_t)W * 8 + 128 * 4 + (size_t)(W + 1) * 8 +
@@ -74,7 +74,7 @@ __device__ inline Beam beam_carve(unsigned char* p, uint32_t W) {
 }
 
 __device__ __forceinline__ uint32_t hslot(uint32_t key, uint32_t mask) {
-  return ((key * 0x9E3779B1u) >> 23) & mask;
+  return ((key * 0x9E3779B1u) >> 22) & mask;
 }
 
 // The reference keeps the beam ids sorted (top_M_Cand2, :1253-1259) only to
