@@ -190,3 +190,25 @@ def test_host_prep_matches_reference_steps(orc):
     c = np.cumsum(base, axis=0, dtype=np.float32)[-1] / np.float32(base.shape[0])
     assert np.array_equal(center, (c.astype(np.float32) * f).astype(np.float16))
     assert np.array_equal(half, (base * f).astype(np.float16))
+
+
+def test_greedy_search_walks_a_line(orc):
+    """NSG's search on a hand-checkable graph: ten points on a line, each
+    linked to its two neighbours. From node 0 with a pool of 3 and no random
+    starts, the search must expand along the line and end with the three
+    nodes nearest to a query past node 9, in distance order; with a pool of
+    1 it still reaches node 9, since every step finds a closer neighbour."""
+    base = np.zeros((10, 4), np.float32)
+    base[:, 0] = np.arange(10)
+    offs, adj = [0], []
+    for i in range(10):
+        adj += [j for j in (i - 1, i + 1) if 0 <= j < 10]
+        offs.append(len(adj))
+    offs = np.array(offs, np.uint64)
+    adj = np.array(adj, np.uint32)
+    q = np.array([[9.4, 0, 0, 0]], np.float32)
+    assert orc.greedy_search(base, offs, adj, 0, q, 3, 3, 0).tolist() == [[9, 8, 7]]
+    assert orc.greedy_search(base, offs, adj, 0, q, 1, 1, 0).tolist() == [[9]]
+    # k past the pool: the slots the pool cannot fill hold 0xFFFFFFFF
+    assert orc.greedy_search(base, offs, adj, 0, q, 2, 4, 0).tolist() == [[9, 8, 0xFFFFFFFF,
+                                                                          0xFFFFFFFF]]
