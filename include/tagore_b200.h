@@ -292,6 +292,14 @@ int tagore_last_screen(TagoreScreenStats* out);
 int tagore_mlp_loss_grad(const uint16_t* rows, uint32_t n, uint32_t dim, const uint32_t* tri,
                          uint32_t B, const float* params, float* grads, double* loss);
 
+/* No counterpart in the reference. Checks on the current device that the
+ * library's bounded waits end instead of hanging: one block holds TMEM and
+ * waits on an mbarrier that nothing ever arrives on, through the same bounded
+ * wait as the tensor-core joins (2 s); when the wait runs out it records it,
+ * frees the TMEM and returns. *timed_out is 1 when that happened; the device
+ * stays usable afterwards. */
+int tagore_wait_selftest(int* timed_out);
+
 /* Frees a device buffer this library allocated (capsule destructor). Like
  * cudaFree it waits for the device's work first. */
 int tagore_device_free(void* p);

@@ -130,6 +130,7 @@ SIGNATURES = {
     "tagore_stage_stats": (C.c_int, [C.POINTER(StageStat), C.c_int, C.POINTER(C.c_int)]),
     "tagore_device_free": (C.c_int, [C.c_void_p]),
     "tagore_trim_cache": (C.c_int, []),
+    "tagore_wait_selftest": (C.c_int, [C.POINTER(C.c_int)]),
     "tagore_last_screen": (C.c_int, [C.POINTER(ScreenStats)]),
     "tagore_mlp_loss_grad": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32,
                                        C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),

@@ -518,6 +518,13 @@ int tagore_entry_point(TagoreKnnState* st, uint32_t topm, uint32_t* ep) {
   return stage_cal_ep(dev_of(st), topm, ep, s.s);
 }
 
+int tagore_wait_selftest(int* timed_out) {
+  if (!timed_out) return fail(TAGORE_EINVAL, "null argument");
+  Stream s;
+  TG_TRY(s.init());
+  return knn::wait_selftest(timed_out, s.s);
+}
+
 int tagore_search(const TagoreSearchParams* p, const float* base, uint64_t n, uint32_t dim,
                   const uint64_t* offs, const uint32_t* adj, uint64_t edges, uint32_t ep,
                   const float* queries, uint32_t nq, uint32_t* out, void* stream) {

@@ -117,6 +117,13 @@ int greedy_search(const TagoreSearchParams& p, const float* base, uint64_t n, ui
                   const uint64_t* offs, const uint32_t* adj, uint64_t edges, uint32_t ep,
                   const float* queries, uint32_t nq, uint32_t* out, cudaStream_t s);
 
+// ---- bounded-wait self-test (knn_tc.cu) ----
+// k_wait_selftest: *timed_out = 1 when the wait on an mbarrier nothing
+// arrives on ran out and the block returned.
+namespace knn {
+int wait_selftest(int* timed_out, cudaStream_t s);
+}
+
 // ---- kNN graph (knn.cu) ----
 struct KnnArgs {
   uint32_t k, iters, mode;  // mode: TAGORE_KNN_CHOSEN / _PLAIN / _LEARNED

@@ -863,6 +863,27 @@ __global__ void __launch_bounds__(kWideThreads, 2)
                  "r"(kWideTmemCols));
 }
 
+// One block that waits, bounded, on an mbarrier nothing arrives on, holding
+// TMEM as the join kernels do: the wait runs out after kWaitNs, the block
+// records it, frees its TMEM and returns.
+__global__ void k_wait_selftest(int* __restrict__ timed_out) {
+  __shared__ __align__(8) unsigned long long bar;
+  __shared__ uint32_t taddr;
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(&taddr)),
+               "r"(32u));
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  __syncwarp();
+  if (threadIdx.x == 0 && !mbar_wait_bounded(smem_u32(&bar), 0)) *timed_out = 1;
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncwarp();
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(32u));
+}
+
 using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -922,6 +943,17 @@ int launch_wide(const Work& w, const CUtensorMap& map, cudaStream_t s) {
 }
 
 }  // namespace
+
+int wait_selftest(int* timed_out, cudaStream_t s) {
+  Scratch flag(s);
+  TG_TRY(flag.alloc(sizeof(int)));
+  TG_CUDA(cudaMemsetAsync(flag.p, 0, sizeof(int), s));
+  k_wait_selftest<<<1, 32, 0, s>>>(flag.as<int>());
+  TG_CUDA(cudaGetLastError());
+  TG_CUDA(cudaMemcpyAsync(timed_out, flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TG_CUDA(cudaStreamSynchronize(s));
+  return TAGORE_OK;
+}
 
 int join_tc_wide(const Work& w, cudaStream_t s) {
   if (!tc_wide_supported(w.dim))
