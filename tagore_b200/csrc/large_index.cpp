@@ -400,13 +400,16 @@ int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int nd
   builder(0);  // the calling thread is builder 0
   for (auto& t : pool) t.join();
   merger.join();
+  // the first error recorded wins: a builder's (with its message), else the merger's
   int rc;
+  std::string msg;
   {
     std::lock_guard<std::mutex> g(sh.mu);
-    rc = merge_rc == TAGORE_OK ? sh.error : TAGORE_OK;
+    rc = sh.error;
+    msg = sh.msg;
   }
-  if (rc != TAGORE_OK) return fail(rc, "%s", sh.msg.c_str());
-  if (merge_rc != TAGORE_OK) return fail(merge_rc, "%s", merge_msg.c_str());
+  if (rc == TAGORE_OK) rc = merge_rc;
+  if (rc != TAGORE_OK) return fail(rc, "%s", msg.empty() ? merge_msg.c_str() : msg.c_str());
   return TAGORE_OK;
 }
 

@@ -70,3 +70,29 @@ def test_large_rejections(capi, tmp_path):
     p.max_degree = 16  # must stay below K
     assert capi.lib().tagore_large_index(C.byref(p), dev, 1) == capi.TAGORE_EINVAL
     assert capi.lib().tagore_large_index(C.byref(p), dev, 2) == capi.TAGORE_EINVAL
+
+
+@pytest.mark.parametrize("missing", [0, 3, 6])
+def test_a_failed_cluster_stops_every_builder(capi, tmp_path, missing):
+    """One cluster's local graph is missing: the builder that takes it fails,
+    the other builder threads and the merger stop, and the call returns the
+    error instead of hanging or writing a partial index."""
+    K = 16
+    first, second, clusters, rows, medoids = scenario(5, K=K)
+    N, Cn = len(first), len(clusters)
+    cpath = tmp_path / "centers.bin"
+    np.stack([first, second], 1).astype(np.uint32).tofile(cpath)
+    p = capi.LargeParams()
+    p.dim, p.k, p.cluster_num, p.max_points = 8, K, Cn, 10_000
+    p.data_prefix = str(tmp_path / "unused_").encode()
+    p.local_prefix = str(tmp_path / "local_").encode()
+    p.index_store_path = str(tmp_path / "final.index").encode()
+    p.max_degree, p.buffer_size, p.num = 10, 3, N
+    p.centers_path = str(cpath).encode()
+    p.thre, p.final_degree, p.topm, p.knn_iters, p.mode = 1.2, 12, 16, 4, 0
+    keep = [np.ascontiguousarray(r) for r in rows]
+    arr = (C.c_void_p * Cn)(*[None if c == missing else keep[c].ctypes.data for c in range(Cn)])
+    meds = np.asarray(medoids, np.uint32)
+    rc = capi.lib().tagore_large_merge(C.byref(p), arr, meds.ctypes.data_as(C.c_void_p))
+    assert rc == capi.TAGORE_EINVAL
+    assert f"no local graph for cluster {missing}".encode() in capi.lib().tagore_last_error()
