@@ -109,15 +109,22 @@ def stage_stats(capi):
             for i in range(min(cnt.value, 32))}
 
 
-def recall_knn(g, half_t, samp, k=10):
+def recall_knn(g, half_t, samp, k=10, batch=2000):
+    """kNN recall@k of rows g on the sampled nodes against brute force over the
+    FP16 base, in batches of sampled nodes."""
     import torch
     x = half_t.float()
-    q = x[samp]
-    d2 = (q * q).sum(1, keepdim=True) + (x * x).sum(1)[None] - 2.0 * (q @ x.T)
-    d2[torch.arange(len(samp)), torch.as_tensor(samp, device=x.device)] = float("inf")
-    truth = torch.topk(d2, k, largest=False).indices.cpu().numpy()
-    return float(np.mean([len(set(g[s, :k].tolist()) & set(truth[i].tolist())) / k
-                          for i, s in enumerate(samp)]))
+    xx = (x * x).sum(1)
+    hits = 0
+    for b in range(0, len(samp), batch):
+        sb = samp[b:b + batch]
+        q = x[sb]
+        d2 = (q * q).sum(1, keepdim=True) + xx[None] - 2.0 * (q @ x.T)
+        d2[torch.arange(len(sb)), torch.as_tensor(sb, device=x.device)] = float("inf")
+        truth = torch.topk(d2, k, largest=False).indices.cpu().numpy()
+        hits += sum(len(set(g[s, :k].tolist()) & set(truth[i].tolist())) for i, s in enumerate(sb))
+        del d2
+    return hits / (k * len(samp))
 
 
 def index_recall(rows, ep, base, queries, half_t, k=10, L=128, seed=0x5EED):
@@ -274,7 +281,7 @@ def main():
 
     extra = {}
     if not a.skip_recall and rank == 0:
-        samp = np.random.default_rng(0).choice(n, 1000, replace=False)
+        samp = np.random.default_rng(0).choice(n, min(n, 10_000), replace=False)
         for label, mode in (("chosen", capi.KNN_CHOSEN), ("plain", capi.KNN_PLAIN)):
             if label == "plain" and a.skip_plain:
                 continue
