@@ -135,7 +135,7 @@ static int device_pool(cudaMemPool_t* out) {
 }
 
 int pool_alloc(void** p, size_t bytes, cudaStream_t s) {
-  cudaMemPool_t pool;
+  cudaMemPool_t pool = nullptr;
   TG_TRY(device_pool(&pool));
   const cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, s);
   if (e != cudaSuccess) {
@@ -412,7 +412,7 @@ int tagore_mlp_loss_grad(const uint16_t* rows, uint32_t n, uint32_t dim, const u
 }
 
 int tagore_trim_cache(void) {
-  cudaMemPool_t pool;
+  cudaMemPool_t pool = nullptr;
   TG_TRY(device_pool(&pool));
   TG_CUDA(cudaDeviceSynchronize());
   TG_CUDA(cudaMemPoolTrimTo(pool, 0));

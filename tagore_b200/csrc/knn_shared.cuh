@@ -142,32 +142,26 @@ __device__ __forceinline__ float thread_dist(const uint32_t* __restrict__ a,
       const uint32_t* r = w ? b : a;
       return make_uint2(r[2 * j], r[2 * j + 1]);
     });
-  }
-  float x[32], y[32];
-#pragma unroll
-  for (int l = 0; l < 32; ++l) {
-    x[l] = 0.0f;
-    y[l] = 0.0f;
-  }
-  if constexpr (D > 0) {
-#pragma unroll
-    for (int j = 0; j < D / 4; ++j)
-      chunk_acc(make_uint2(a[2 * j], a[2 * j + 1]), make_uint2(b[2 * j], b[2 * j + 1]),
-                x[j & 31], y[j & 31]);
   } else {
+    float x[32], y[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) {
+      x[l] = 0.0f;
+      y[l] = 0.0f;
+    }
     for (uint32_t j = 0; j < dim_rt / 4; ++j)
       chunk_acc(make_uint2(a[2 * j], a[2 * j + 1]), make_uint2(b[2 * j], b[2 * j + 1]),
                 x[j & 31], y[j & 31]);
-  }
 #pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
+    for (int off = 16; off > 0; off >>= 1) {
 #pragma unroll
-    for (int l = 0; l < off; ++l) {
-      x[l] = __fadd_rn(x[l], x[l + off]);
-      y[l] = __fadd_rn(y[l], y[l + off]);
+      for (int l = 0; l < off; ++l) {
+        x[l] = __fadd_rn(x[l], x[l + off]);
+        y[l] = __fadd_rn(y[l], y[l + off]);
+      }
     }
+    return __fadd_rn(x[0], y[0]);
   }
-  return __fadd_rn(x[0], y[0]);
 }
 
 }  // namespace knn

@@ -509,7 +509,6 @@ constexpr int kWideRing = 6;                       // column blocks in flight
 constexpr int kWideNodes = 2;                      // node metadata slots
 constexpr int kWideThreads = kConsumers + 64;      // consumers, producer (warp 4), MMA (warp 5)
 constexpr uint32_t kWideTmemCols = 256;            // two 128-column accumulators
-constexpr uint32_t kWideMaxDim = 1024;
 
 struct __align__(1024) WideSmem {
   uint8_t ring[kWideRing][kMaxList][128];  // one column block: [row][128 B], SW128

@@ -30,7 +30,6 @@ namespace {
 
 constexpr int kWarps = 4;  // warps (= nodes in flight) per block
 
-__device__ __forceinline__ uint32_t align4(uint32_t x) { return (x + 3u) & ~3u; }
 
 // ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
