@@ -43,15 +43,17 @@ struct Beam {
   float* dis;
   uint8_t* ex;
   uint32_t* hash;  // membership set of the W beam ids (open addressing)
-  uint32_t hmask;  // hash slots - 1
+  uint32_t hslots;  // hash slots
   float* sb;       // scratch (K): the fresh positions, then sorted entering distances
   float* sm;       // staging (W + 1): merged distances of positions 0..TOPM
   uint32_t* sid;   // staging (W + 1): their ids
   uint8_t* sex;    // staging (W + 1): their explored flags
 };
 
-// Hash slots: a power of two holding the beam at load <= 3/8 (TOPM <= 256, K <= 128).
-__host__ __device__ inline uint32_t hash_slots(uint32_t W) { return W <= 192 ? 512u : 1024u; }
+// Hash slots: the beam at load <= 1/2 (TOPM <= 256, K <= 128). 384 slots keep a
+// warp's beam region within its candidate list's, so six blocks per SM still
+// fit the 132 KB shared-memory carveout and leave L1 its larger share.
+__host__ __device__ inline uint32_t hash_slots(uint32_t W) { return W <= 192 ? 384u : 768u; }
 
 __host__ __device__ inline size_t beam_bytes(uint32_t W) {
   return (size_t)hash_slots(W) * 4 + (size_t)W * 8 + 128 * 4 + (size_t)(W + 1) * 8 +
@@ -61,7 +63,7 @@ __host__ __device__ inline size_t beam_bytes(uint32_t W) {
 __device__ inline Beam beam_carve(unsigned char* p, uint32_t W) {
   Beam b;
   b.hash = reinterpret_cast<uint32_t*>(p);
-  b.hmask = hash_slots(W) - 1;
+  b.hslots = hash_slots(W);
   b.id = b.hash + hash_slots(W);
   b.dis = reinterpret_cast<float*>(b.id + W);
   b.sb = b.dis + W;
@@ -72,36 +74,36 @@ __device__ inline Beam beam_carve(unsigned char* p, uint32_t W) {
   return b;
 }
 
-__device__ __forceinline__ uint32_t hslot(uint32_t key, uint32_t mask) {
-  return ((key * 0x9E3779B1u) >> 22) & mask;
+__device__ __forceinline__ uint32_t hslot(uint32_t key, uint32_t slots) {
+  return (uint32_t)(((uint64_t)(key * 0x9E3779B1u) * slots) >> 32);  // multiply-shift into [0, slots)
 }
 
 // The reference keeps the beam ids sorted (top_M_Cand2, :1253-1259) only to
 // test membership (:1282-1290); a hash set of the same ids answers the same
 // question without a sort.
 __device__ __noinline__ void beam_rehash(Beam bm, uint32_t W, int lane) {
-  for (uint32_t t = lane; t <= bm.hmask; t += 32) bm.hash[t] = kInv;
+  for (uint32_t t = lane; t < bm.hslots; t += 32) bm.hash[t] = kInv;
   __syncwarp();
   for (uint32_t t = lane; t < W; t += 32) {
     const uint32_t key = bm.id[t];
     if (key == kInv) continue;
-    uint32_t h = hslot(key, bm.hmask);
+    uint32_t h = hslot(key, bm.hslots);
     while (true) {
       const uint32_t prev = atomicCAS(&bm.hash[h], kInv, key);
       if (prev == kInv || prev == key) break;
-      h = (h + 1) & bm.hmask;
+      h = h + 1 == bm.hslots ? 0u : h + 1;
     }
   }
   __syncwarp();
 }
 
 __device__ __forceinline__ bool beam_has(const Beam& bm, uint32_t key) {
-  uint32_t h = hslot(key, bm.hmask);
+  uint32_t h = hslot(key, bm.hslots);
   while (true) {
     const uint32_t v = bm.hash[h];
     if (v == key) return true;
     if (v == kInv) return false;
-    h = (h + 1) & bm.hmask;
+    h = h + 1 == bm.hslots ? 0u : h + 1;
   }
 }
 
