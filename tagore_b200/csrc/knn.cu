@@ -118,14 +118,34 @@ __global__ void __launch_bounds__(128)
 
 // Join list of each node: forward new, reverse new (deduped, first kept),
 // then forward old and reverse old not already present. Warp per node.
+// Repeats are found with a per-warp open-addressing table of the node's up to
+// 128 entries (256 slots, load <= 1/2): every entry claims its id's slot, and
+// the slot's owner is the smallest position (source-major, then lane) that
+// holds the id, so the first copy is the one kept whatever the order in which
+// the lanes' atomics land.
+constexpr uint32_t kListSlots = 256;
+
+__device__ __forceinline__ uint32_t list_slot(uint32_t* __restrict__ key, uint32_t id) {
+  uint32_t h = (id * 0x9E3779B1u) >> 24;  // 8 bits: kListSlots == 256
+  for (uint32_t p = 0; p < kListSlots; ++p) {
+    const uint32_t prev = atomicCAS(&key[h], kInv, id);
+    if (prev == kInv || prev == id) break;
+    h = (h + 1) & (kListSlots - 1);
+  }
+  return h;  // at most 128 ids in 256 slots: the loop ends on a free or own slot
+}
+
 __global__ void __launch_bounds__(128)
     k_build_lists(uint32_t n, uint32_t S, const uint32_t* __restrict__ fnew,
                   const uint32_t* __restrict__ fold, const uint32_t* __restrict__ fcnt,
                   const uint32_t* __restrict__ rnew, const uint32_t* __restrict__ rold,
                   const uint32_t* __restrict__ rcnt, uint32_t* __restrict__ lists,
                   uint32_t* __restrict__ lcnt) {
+  __shared__ __align__(16) uint32_t key_s[4][kListSlots], owner_s[4][kListSlots];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
+  uint32_t* key = key_s[warp];
+  uint32_t* owner = owner_s[warp];
   for (uint32_t u = blockIdx.x * 4 + warp; u < n; u += gridDim.x * 4) {
     // the four sources, one entry per lane (S <= 32): forward new, reverse
     // new, forward old, reverse old -- the order in which repeats keep their
@@ -137,27 +157,36 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
     for (int q = 0; q < 4; ++q)
       x[q] = (uint32_t)lane < cnt[q] ? src[q][(size_t)u * S + lane] : kInv;
-    // an entry is kept when it is not u and no earlier entry holds its id:
-    // earlier lanes of its own source (match), then every earlier source
-    bool keep[4];
+    const uint4 none = make_uint4(kInv, kInv, kInv, kInv);
+#pragma unroll
+    for (uint32_t t = (uint32_t)lane; t < kListSlots / 4; t += 32) {
+      reinterpret_cast<uint4*>(key)[t] = none;
+      reinterpret_cast<uint4*>(owner)[t] = none;
+    }
+    __syncwarp();
+    uint32_t slot[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const unsigned same = __match_any_sync(kFull, x[q]);
-      bool dup = (same & lt) != 0u;
-#pragma unroll
-      for (int q2 = 0; q2 < q; ++q2)
-        for (uint32_t j = 0; j < cnt[q2]; ++j) dup |= __shfl_sync(kFull, x[q2], j) == x[q];
-      keep[q] = (uint32_t)lane < cnt[q] && x[q] != u && !dup;
+      slot[q] = 0;
+      if (x[q] != kInv) {
+        slot[q] = list_slot(key, x[q]);
+        atomicMin(&owner[slot[q]], (uint32_t)(q * 32 + lane));
+      }
     }
+    __syncwarp();
+    // an entry is kept when it is not u and is its id's first copy
     uint32_t pos = 0;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const unsigned m = __ballot_sync(kFull, keep[q]);
-      if (keep[q]) lists[(size_t)u * kMaxList + pos + __popc(m & lt)] = x[q];
+      const bool keep =
+          x[q] != kInv && x[q] != u && owner[slot[q]] == (uint32_t)(q * 32 + lane);
+      const unsigned m = __ballot_sync(kFull, keep);
+      if (keep) lists[(size_t)u * kMaxList + pos + __popc(m & lt)] = x[q];
       pos += __popc(m);
       if (q == 1 && lane == 0) lcnt[2 * u] = pos;  // the new entries
     }
     if (lane == 0) lcnt[2 * u + 1] = pos;
+    __syncwarp();  // every lane has read the table before the next node clears it
   }
 }
 
