@@ -62,7 +62,7 @@ typedef struct TagoreKnnParams {
   uint32_t n;        /* POINTS; the fvecs loader takes the count from the file */
   uint32_t dim;      /* DIM */
   uint32_t iters;    /* iterations; the reference runs iters/2 + iters/2 */
-  uint32_t mode;     /* TAGORE_KNN_CHOSEN or TAGORE_KNN_PLAIN */
+  uint32_t mode;     /* TAGORE_KNN_CHOSEN, TAGORE_KNN_PLAIN or TAGORE_KNN_LEARNED */
   uint32_t sample;   /* forward samples per list and iteration (0: 32) */
   uint32_t per_row;  /* proposals kept per local-join row (0: default) */
   uint32_t rescale;  /* 1: power-of-ten rescale as GNN_descent; 0: none (largeIndex) */
