@@ -122,9 +122,10 @@ int tagore_pruning_cfs(const TagorePruneParams* p, TagoreKnnState* st, const cha
  * TAGORE_EINVAL. Work goes to `stream` (a cudaStream_t; NULL is the legacy
  * default stream) and the call returns after it has finished. Calls that
  * overlapped on the GPU would race on the shared array; calls are serialised
- * by a process-wide lock. The first call on a device does its set-up (module
- * load, symbol lookup, kernel attributes) and should come before any stream
- * capture. */
+ * by a process-wide lock, and each call waits for its work on `stream`
+ * before it returns, on error paths too. The first call on a device does its
+ * set-up (module load, symbol lookup, kernel attributes) and should come
+ * before any stream capture. */
 int tagore_pruning_cfs_noalloc(const TagorePruneParams* p, TagoreKnnState* st, const char* mode,
                                const char* metric, void* stream);
 
@@ -299,6 +300,11 @@ int tagore_mlp_loss_grad(const uint16_t* rows, uint32_t n, uint32_t dim, const u
  * frees the TMEM and returns. *timed_out is 1 when that happened; the device
  * stays usable afterwards. */
 int tagore_wait_selftest(int* timed_out);
+
+/* No counterpart in the reference. How many allocations this library has
+ * made since it was loaded: device memory from its pools and pinned host
+ * buffers. A call that allocates nothing leaves it unchanged. */
+uint64_t tagore_allocation_count(void);
 
 /* Frees a device buffer this library allocated (capsule destructor). Like
  * cudaFree it waits for the device's work first. */

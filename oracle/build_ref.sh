@@ -5,8 +5,10 @@
 # The reference includes <boost/dynamic_bitset.hpp> for dead CPU code only
 # (src/common.cu:65-148); a small stand-in header is written instead.
 set -e
-REF=${TAGORE_REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# The reference sources: TAGORE_REF, else a `reference` folder beside the repository.
+REF=${TAGORE_REF:-$HERE/../../reference}
+[ -d "$REF/src" ] || { echo "reference sources not found at $REF (set TAGORE_REF)"; exit 1; }
 OUT="$HERE/_ref"
 mkdir -p "$OUT/include/boost"
 cat > "$OUT/include/boost/dynamic_bitset.hpp" <<'HDR'

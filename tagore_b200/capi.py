@@ -129,6 +129,7 @@ SIGNATURES = {
     "tagore_set_profiling": (C.c_int, [C.c_int]),
     "tagore_stage_stats": (C.c_int, [C.POINTER(StageStat), C.c_int, C.POINTER(C.c_int)]),
     "tagore_device_free": (C.c_int, [C.c_void_p]),
+    "tagore_allocation_count": (C.c_uint64, []),
     "tagore_trim_cache": (C.c_int, []),
     "tagore_wait_selftest": (C.c_int, [C.POINTER(C.c_int)]),
     "tagore_last_screen": (C.c_int, [C.POINTER(ScreenStats)]),

@@ -43,6 +43,11 @@ static TagoreStageStat& stat_of(const char* name) {
 }
 
 void count_launch(uint32_t n) { g_launches += n; }
+
+// Every device or pinned-host allocation the library makes goes through
+// pool_alloc or count_allocation, so this count sees all of them.
+static std::atomic<uint64_t> g_allocs{0};
+void count_allocation() { ++g_allocs; }
 bool profiling() { return g_prof; }
 
 void stage_begin(const char* name, cudaStream_t s) {
@@ -135,6 +140,7 @@ static int device_pool(cudaMemPool_t* out) {
 }
 
 int pool_alloc(void** p, size_t bytes, cudaStream_t s) {
+  count_allocation();
   cudaMemPool_t pool = nullptr;
   TG_TRY(device_pool(&pool));
   const cudaError_t e = cudaMallocFromPoolAsync(p, bytes, pool, s);
@@ -291,6 +297,8 @@ int tagore_last_timings(TagoreTimings* t) {
   t->kernel_launches = g_launches.load();
   return TAGORE_OK;
 }
+
+uint64_t tagore_allocation_count(void) { return g_allocs.load(); }
 
 int tagore_reset_counters(void) {
   g_launches = 0;

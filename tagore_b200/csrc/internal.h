@@ -63,6 +63,9 @@ inline Dev dev_of(const TagoreKnnState* s) {
 // memory cached, so repeated builds map no new pages;
 // tagore_trim_cache() gives the cached memory back.
 int pool_alloc(void** p, size_t bytes, cudaStream_t s);
+// Counts one allocation (pool_alloc counts its own; pinned host buffers call
+// this), reported by tagore_allocation_count().
+void count_allocation();
 void pool_free(void* p, cudaStream_t s);
 
 // Stream-ordered scratch from the device pool, released on the same stream.

@@ -170,6 +170,7 @@ int ingest_fvecs(const char* path, uint32_t n, uint32_t dim, bool rescale, float
     }
   } release{pinned, ev};
   for (int i = 0; i < 2; ++i) {
+    count_allocation();
     TG_CUDA(cudaMallocHost(&pinned[i], chunk_bytes));
     TG_CUDA(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
   }

@@ -1276,6 +1276,14 @@ int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
   Carve c{static_cast<unsigned char*>(base)};
   layout(c, &flags, &P_ids, &P_dis, &P_cnt, &keys, &vals, &keys2, &vals2, &deg, &off, &tmp_p);
 
+  // From the first queued operation on, every return waits for the stream,
+  // so the caller's lock is released only when no work on the shared array
+  // is still in flight, error paths included.
+  struct DrainOnExit {
+    cudaStream_t s;
+    ~DrainOnExit() { cudaStreamSynchronize(s); }
+  } drain{s};
+
   // validate (as validate())
   TG_CUDA(cudaMemsetAsync(flags, 0, 16, s));
   const size_t cnt = (size_t)d.n * d.k;
