@@ -50,6 +50,7 @@ def lib():
             "orc_greedy_search": (C.c_int, [vp, u32, u32, vp, vp, u32, vp, u32, u32, u32, C.c_uint64, vp]),
             "orc_nndescent": (C.c_int, [vp, u32, u32, u32, u32, u32, C.c_uint64, vp, vp]),
             "orc_num_threads": (C.c_int, []),
+            "orc_gnn_descent_model": (C.c_int, [vp, u32, u32, u32, u32, C.c_uint64, vp, vp]),
         }
         for name, (res, args) in sigs.items():
             fn = getattr(L, name)
@@ -176,6 +177,19 @@ def nndescent(base, k, iters, sample=32, seed=0x7A6E):
     rc = lib().orc_nndescent(_p(base), n, dim, k, iters, sample, seed, _p(ids), _p(dis))
     if rc:
         raise ValueError("bad nndescent arguments")
+    return ids, dis
+
+
+def gnn_descent_model(data_f16, K, iters, seed=0x7A6E):
+    """The reference's two-phase GNN_descent restated on the CPU
+    (gnn_descent_model.cpp): returns (ids, dists), each n x K."""
+    data = np.ascontiguousarray(data_f16, dtype=np.float16)
+    n, dim = data.shape
+    ids = np.empty((n, K), np.uint32)
+    dis = np.empty((n, K), np.float32)
+    rc = lib().orc_gnn_descent_model(_p(data), n, dim, K, iters, seed, _p(ids), _p(dis))
+    if rc:
+        raise ValueError("gnn_descent_model needs K in {32, 64, 96}, dim % 4 == 0 and n > K")
     return ids, dis
 
 

@@ -11,7 +11,10 @@ Inputs are chosen so the reference is deterministic where it can be:
     its own row), reverse lists that never overflow.
 Each prune case runs three times on fresh buffers; an output that differs
 between runs (the reference's cross-block races) is stored as unstable.
-Outputs: OUTDIR/golden_prune.npz and OUTDIR/golden_prep.npz.
+A second set of cases runs on a base of quarter values (non-integer, still
+exact in FP16) at a larger degree, with NSSG and CAGRA index files.
+Outputs: OUTDIR/golden_prune.npz, OUTDIR/golden_prune_quarter.npz and
+OUTDIR/golden_prep.npz.
 """
 import ctypes
 import os
@@ -84,6 +87,66 @@ def run_reference(T, torch, x, center, call):
     return ids, dis, res
 
 
+def distinct_quarter_base(seed=17, n=N, d=D):
+    """Like distinct_integer_base, on multiples of 1/4 in [0, 2.5]: every
+    difference, square and partial sum is a multiple of 1/16 below 128, so the
+    reference's FP16 arithmetic is exact and equals the oracle's FP32."""
+    rng = np.random.default_rng(seed)
+    pts = [rng.integers(0, 11, size=d) / 4.0]
+    dists = [set()]
+    while len(pts) < n:
+        c = rng.integers(0, 11, size=d) / 4.0
+        dd = [float(((c - p) ** 2).sum()) for p in pts]
+        if len(set(dd)) != len(dd) or max(dd) >= 128 or min(dd) == 0:
+            continue
+        if any(dd[i] in dists[i] for i in range(len(pts))):
+            continue
+        for i in range(len(pts)):
+            dists[i].add(dd[i])
+        dists.append(set(dd))
+        pts.append(c)
+    return np.array(pts, np.float32)
+
+
+QFD = 16  # a larger degree than the integer cases, so most filter_reverse rows take the union branch
+
+
+def quarter_cases(T, torch, outdir, tmp):
+    """NSG, Vamana, NSSG (2-hop + angle at 60 degrees) and CAGRA, each with its
+    index file, on the quarter-valued base. DPG is left out: its four warps
+    share one staging vector (src/Tagore_src.cu:1715-1720) and its writer takes
+    each row's count from the dense rows (src/common.cu:219-237), so its output
+    pins nothing."""
+    x = distinct_quarter_base()
+    rng = np.random.default_rng(19)
+    while True:
+        center = rng.integers(0, 11, size=D) / 4.0
+        dc = ((x - center) ** 2).sum(1)
+        if len(set(dc.tolist())) == N and dc.min() > 0 and dc.max() < 128:
+            break
+    center = center.astype(np.float32)
+
+    def file_call(kind, thre):
+        def call(T, ptrs):
+            path = os.path.join(tmp, f"q_{kind}.index")
+            T.Pruning(K, N, D, QFD, TOPM, ptrs, kind, thre, path)
+            return open(path, "rb").read()
+        return call
+
+    cases = {"nsg": file_call("NSG", 1.0), "vamana": file_call("Vamana", 1.2),
+             "nssg": file_call("NSSG", 0.5), "cagra": file_call("CAGRA", 1.0)}
+    arrays = {"x": x, "center": center, "meta": np.array([N, D, K, QFD, TOPM], np.int64)}
+    for name, call in cases.items():
+        runs = [run_reference(T, torch, x, center, call)[2] for _ in range(3)]
+        for key in runs[0]:
+            vals = [r[key] for r in runs]
+            stable = all(np.array_equal(vals[0], v) for v in vals[1:])
+            arrays[f"{name}/{key}"] = vals[0]
+            arrays[f"{name}/{key}/stable"] = np.array(stable)
+            print("quarter", name, key, "stable" if stable else "UNSTABLE", flush=True)
+    np.savez_compressed(os.path.join(outdir, "golden_prune_quarter.npz"), **arrays)
+
+
 def main():
     outdir = sys.argv[1]
     os.makedirs(outdir, exist_ok=True)
@@ -127,6 +190,7 @@ def main():
             arrays[f"{name}/{key}/stable"] = np.array(stable)
             print(name, key, "stable" if stable else "UNSTABLE", flush=True)
     np.savez_compressed(os.path.join(outdir, "golden_prune.npz"), **arrays)
+    quarter_cases(T, torch, outdir, tmp)
 
     # Host preparation of GNN_descent: FP16 base and centre (capsules 2 and 6).
     from tagore_b200 import synth

@@ -1,6 +1,7 @@
 """The CPU oracle against golden outputs of the reference Tagore module itself
 (tests/golden/make_golden.py ran it on a B200, three times per case; outputs
-that differed between its runs are skipped).
+that differed between its runs are skipped). A second fixture repeats NSG and
+Vamana and adds NSSG and CAGRA on a base of quarter values, at degree 16.
 
 What the reference fixes and the oracle must match exactly: the select stage
 (nei_distance rows, reverse counts), the entry point, every row filled by the
@@ -107,6 +108,78 @@ def test_oracle_matches_reference(orc, name):
             rows = parse_rows(np.frombuffer(raw[24:], np.uint32), 0, n)
         for u in range(n):
             assert sorted(rows[u]) == sorted(got[u, 1:1 + got[u, 0]].tolist()), f"file row {u}"
+
+
+QUARTER = os.path.join(HERE, "golden", "golden_prune_quarter.npz")
+QCASES = {"nsg": ("path", 0, 1.0, "NSG"), "vamana": ("path", 0, 1.2, "Vamana"),
+          "nssg": ("2-hop", 1, 0.5, "NSSG")}
+
+
+@pytest.mark.parametrize("name", list(QCASES))
+def test_oracle_matches_reference_quarter_base(orc, name):
+    """Non-integer base, degree 16. For NSSG (2-hop collect with the angle
+    filter at 60 degrees) the rows that filter_reverse re-prunes are skipped:
+    there the reference reads an angle of an unset shared variable
+    (cur_nei_dis, src/Tagore_src.cu:1545); rows it unites with their reverse
+    edges carry the select stage's angle-filtered lists unchanged."""
+    g = load(QUARTER)
+    n, d, k, fd, topm = [int(v) for v in g["meta"]]
+    collect, metric, thre, kind = QCASES[name]
+    buf, sel_deg, ep = run_stages(orc, g, collect, metric, thre)
+    rnum = buf.reverse_num
+    for key in ("nei_distance", "reverse_num"):
+        assert bool(g[f"{name}/{key}/stable"]), key
+        assert np.array_equal(g[f"{name}/{key}"].view(np.uint32),
+                              getattr(buf, key).view(np.uint32)), key
+    union = sel_deg.astype(np.int64) + np.minimum(k, rnum.astype(np.int64)) <= fd
+    ref_rows = g[f"{name}/graph"].reshape(n, k)
+    got = buf.graph.reshape(n, k)
+    if metric == 1:
+        assert union.sum() >= n // 2, "too few union rows to pin the angle filter"
+        keep = np.nonzero(union)[0]
+        compare_rows(ref_rows[keep], got[keep], sel_deg[keep], rnum[keep], fd, k)
+    else:
+        compare_rows(ref_rows, got, sel_deg, rnum, fd, k)
+    raw = g[f"{name}/file"].tobytes()
+    if kind == "NSG":
+        assert struct.unpack("<II", raw[:8]) == (fd, ep)
+        rows = parse_rows(np.frombuffer(raw[8:], np.uint32), 0, n)
+    elif kind == "Vamana":
+        size, maxd, ref_ep, frozen = struct.unpack("<QIIQ", raw[:24])
+        assert (size, ref_ep, frozen, maxd) == (len(raw), ep, 0, int(got[:, 0].max()))
+        rows = parse_rows(np.frombuffer(raw[24:], np.uint32), 0, n)
+    else:  # NSSG: width, 10 random entry points (unseeded shuffle), rows
+        width, n_ep = struct.unpack("<II", raw[:8])
+        assert (width, n_ep) == (fd, 10)
+        eps = np.frombuffer(raw[8:48], np.uint32)
+        assert len(set(eps.tolist())) == 10 and eps.max() < n
+        rows = parse_rows(np.frombuffer(raw[48:], np.uint32), 0, n)
+    for u in range(n):
+        if metric == 1 and not union[u]:
+            continue
+        assert sorted(rows[u]) == sorted(got[u, 1:1 + got[u, 0]].tolist()), f"file row {u}"
+
+
+def test_cagra_file_and_forward_lists_quarter_base(orc):
+    """CAGRA on the quarter base: the detour-ranked forward half of every row,
+    the select stage's lists and counts, and the file layout {[u32 d][d ids]}
+    (src/common.cu:240-248) against the reference's file."""
+    g = load(QUARTER)
+    n, d, k, fd, topm = [int(v) for v in g["meta"]]
+    ids, dis = exact_knn(g["x"], k)
+    buf = orc.Buffers(ids, dis, g["x"].astype(np.float16))
+    orc.prune(buf, fd, "CAGRA")
+    for key in ("hybrid_list", "reverse_num"):
+        assert bool(g[f"cagra/{key}/stable"]), key
+        assert np.array_equal(g[f"cagra/{key}"], getattr(buf, key)), key
+    got = buf.graph.reshape(-1)[:n * fd].reshape(n, fd)
+    ref = g["cagra/graph"].reshape(-1)[:n * fd].reshape(n, fd)
+    assert np.array_equal(ref[:, :fd // 2], got[:, :fd // 2])
+    raw = np.frombuffer(g["cagra/file"].tobytes(), np.uint32).reshape(n, fd + 1)
+    assert (raw[:, 0] == fd).all()
+    assert np.array_equal(raw[:, 1:], ref)
+    for u in range(n):
+        assert set(raw[u, 1:].tolist()) <= set(ids[u].tolist()) | set(range(n))
 
 
 def test_cagra_forward_lists_match_reference(orc):

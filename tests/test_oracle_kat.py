@@ -6,7 +6,7 @@
   reference's loop (src/Tagore_src.cu:29-44) and compared on inputs with ties.
 * A line graph, whose NSG prune keeps exactly the nearest neighbour on each
   side of every node, gives hand-derived prune results.
-* CAGRA detour counts are recomputed from their definition.
+* CAGRA and DPG detour counts are recomputed from their definitions.
 * The host preparation follows pybind.cu:24-61 step by step.
 """
 import math
@@ -173,6 +173,36 @@ def test_cagra_forward_lists_follow_detour_counts(orc):
         assert hyb[u, :d].tolist() == order[:d]
 
 
+def dpg_detours(orc, x, ids, dis, u, K):
+    """DPG's detour rule (src/Tagore_src.cu:1713-1785) from its definition: for
+    the i-th nearest and the i-th farthest neighbour a (i < K/2), every later
+    neighbour m of the row counts one detour when d(a, m) < d(u, m); the near
+    one is compared with every m after it, the far one with the i entries
+    after it. Each warp of the rule stages its own vector a."""
+    nei0 = ids[u]
+    det = [0] * K
+    for i in range(K // 2):
+        for a, later in ((i, range(i + 1, K)), (K - 1 - i, range(K - i, K))):
+            for m in later:
+                if orc.dist(x[nei0[a]], x[nei0[m]]) < dis[u, m]:
+                    det[m] += 1
+    return det
+
+
+def test_dpg_forward_lists_follow_detour_counts(orc):
+    rng = np.random.default_rng(5)
+    n, K, d = 120, 40, 24
+    x = (rng.random((n, 16)) * 2).astype(np.float16)
+    ids, dis = orc.knn_input(x, K)
+    buf = orc.Buffers(ids, dis, x)
+    orc.prune(buf, d, "DPG")
+    hyb = buf.hybrid_list[:n * K].reshape(n, K)
+    for u in range(0, n, 5):
+        det = dpg_detours(orc, x, ids, dis, u, K)
+        _, order = py_network(det, list(ids[u]))
+        assert hyb[u, :d].tolist() == order[:d], u
+
+
 def test_host_prep_matches_reference_steps(orc):
     from tagore_b200 import synth
     base, _ = synth.mixture("sift", 3000, 128, 8, 11)
@@ -212,3 +242,20 @@ def test_greedy_search_walks_a_line(orc):
     # k past the pool: the slots the pool cannot fill hold 0xFFFFFFFF
     assert orc.greedy_search(base, offs, adj, 0, q, 2, 4, 0).tolist() == [[9, 8, 0xFFFFFFFF,
                                                                           0xFFFFFFFF]]
+
+
+def test_reference_gnn_descent_model_runs(orc):
+    """The CPU model of the reference's GNN_descent: sorted rows of valid,
+    non-self ids whose recall is well above chance after two iterations."""
+    from tagore_b200 import synth
+    n, d, K = 2000, 128, 32
+    base, _ = synth.mixture("sift", n, d, 8, 13)
+    half, _, _ = orc.host_prep(base)
+    ids, dis = orc.gnn_descent_model(half.reshape(n, d), K, 2)
+    assert ids.max() < n and not (ids == np.arange(n)[:, None]).any()
+    assert (np.diff(dis, axis=1) >= 0).all()
+    gt = orc.bruteforce_knn(base, base, 10, exclude_self=np.arange(n, dtype=np.uint32))
+    hit = (ids[:, :10, None] == gt[:, None, :]).any(-1).sum(1).mean() / 10
+    assert hit > 0.5
+    with pytest.raises(ValueError):
+        orc.gnn_descent_model(half.reshape(n, d), 40, 2)

@@ -19,7 +19,6 @@ iterations). The recall of both kNN graphs on that input is recorded.
 import ctypes
 import glob
 import importlib.machinery
-import importlib.util
 import os
 
 import numpy as np
@@ -37,11 +36,27 @@ N, D, K, ITERS, FD, TOPM = 2000, 128, 96, 2, 32, 64
 
 
 def load_reference():
+    """The reference's module beside this library's, in one process. Both are
+    pybind11 modules named `Tagore`, and pybind11 hands a second import of a
+    name back the module it cached under that name. So the reference's
+    PyModuleDef (multi-phase init) is instantiated here under its own spec
+    name, as the import system would do it."""
     path = REF_SO[0]
-    loader = importlib.machinery.ExtensionFileLoader("Tagore", path)
-    spec = importlib.util.spec_from_file_location("Tagore", path, loader=loader)
-    mod = importlib.util.module_from_spec(spec)
-    loader.exec_module(mod)
+    api = ctypes.pythonapi
+    init = ctypes.PyDLL(path).PyInit_Tagore
+    init.restype = ctypes.py_object
+    mdef = init()
+    api.Py_IncRef.argtypes = [ctypes.py_object]
+    api.Py_IncRef(mdef)  # a static object: ctypes must never release it
+    api.PyModule_FromDefAndSpec2.restype = ctypes.py_object
+    api.PyModule_FromDefAndSpec2.argtypes = [ctypes.py_object, ctypes.py_object, ctypes.c_int]
+    api.PyModule_ExecDef.restype = ctypes.c_int
+    api.PyModule_ExecDef.argtypes = [ctypes.py_object, ctypes.py_object]
+    spec = importlib.machinery.ModuleSpec("Tagore_reference", None, origin=path)
+    mod = api.PyModule_FromDefAndSpec2(mdef, spec, 1013)
+    mod.__spec__ = spec
+    mod.__file__ = path
+    assert api.PyModule_ExecDef(mod, mdef) == 0
     return mod
 
 
@@ -141,11 +156,20 @@ def test_our_tuple_into_reference_pruning(capi, orc, modules, fvecs, tmp_path):
 
 
 def test_knn_recall_against_reference_same_input(orc, modules, fvecs, capi):
-    """Recall@10 of both GNN_descent graphs on the same file at equal iterations."""
+    """Recall@10 of both GNN_descent graphs on the same file at equal
+    iterations, and of the CPU model of the reference's algorithm
+    (oracle/gnn_descent_model.cpp), which stands in for the reference on
+    inputs it does not run on: the model must land within 0.01 of the
+    reference (both are nondeterministic)."""
     ours, ref = modules
     base, path = fvecs
-    r_ref = knn_recall10(orc, base, host_buffers(capi, ref.GNN_descent(K, N, D, ITERS, path))["graph"])
+    r_ref = [knn_recall10(orc, base, host_buffers(capi, ref.GNN_descent(K, N, D, ITERS, path))["graph"])
+             for _ in range(3)]
     r_our = knn_recall10(orc, base, host_buffers(capi, ours.GNN_descent(K, N, D, ITERS, path))["graph"])
+    half, _, _ = orc.host_prep(base)
+    r_model = [knn_recall10(orc, base, orc.gnn_descent_model(half.reshape(N, D), K, ITERS, seed=s)[0])
+               for s in (1, 2, 3)]
     print(f"kNN recall@10 at {N}x{D}, K={K}, {ITERS} iterations: ours {r_our:.4f}, "
-          f"reference {r_ref:.4f}")
-    assert r_our >= r_ref - 0.002
+          f"reference {np.round(r_ref, 4).tolist()}, model {np.round(r_model, 4).tolist()}")
+    assert r_our >= np.mean(r_ref) - 0.002
+    assert abs(np.mean(r_model) - np.mean(r_ref)) < 0.01
