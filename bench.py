@@ -42,6 +42,7 @@ def args_():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-recall", action="store_true")
+    ap.add_argument("--skip-prunes", action="store_true")
     return ap.parse_args()
 
 
@@ -51,6 +52,26 @@ def peaks():
             return json.load(f)["hbm_gbs"], "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def tensor_peak():
+    """Dense bf16/fp16 tensor peak (TFLOP/s), burst figure: the join is timed alone per launch."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)["bf16_tflops"]
+    except Exception:
+        return 1590.0
+
+
+# What limits each kernel, from its ncu captures (profiles/): the roofline
+# class stays the HBM roofline of a gather kernel, this names the binding.
+BINDING = {
+    "prune_select_path": "latency: dependent L2-hit row gathers per warp step (long_scoreboard); "
+                         "DRAM traffic well below the HBM roofline",
+    "knn_join_tc": "latency and barriers: per-node TMA gathers from L2 and the consumer "
+                   "barriers; tensor pipe lightly used",
+    "knn_merge": "latency: dependent pool loads and global atomics per node",
+}
 
 
 class Clocks:
@@ -270,18 +291,71 @@ def main():
     if not a.skip_plain:
         plain_ms, _, _, _ = timed(capi.KNN_PLAIN, max(1, a.steps // 2), 1)
 
-    # dominant stage -> roofline (algorithmic bytes per launch / mean launch time)
-    name, (s_ms, s_launch, s_bytes, s_items) = max(stages.items(), key=lambda kv: kv[1][0])
+    # per-kernel rooflines (algorithmic bytes per launch / mean launch time)
     peak, peak_kind = peaks()
-    achieved = (s_bytes / max(1, s_launch)) / ((s_ms / max(1, s_launch)) * 1e-3) / 1e9 if s_bytes else None
-    traffic = None
+    tflops_peak = tensor_peak()
     tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        traffic = json.load(open(tf)).get(name)
+    traffic_tab = json.load(open(tf)) if os.path.exists(tf) else {}
+
+    def roofline(name):
+        s_ms, s_launch, s_bytes, _ = stages[name]
+        ms_l = s_ms / max(1, s_launch)
+        byt = s_bytes / max(1, s_launch)
+        achieved = byt / (ms_l * 1e-3) / 1e9 if s_bytes else None
+        traffic = traffic_tab.get(name)
+        r = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+             "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+             "traffic": traffic, "algorithmic_bytes_per_launch": byt, "ms_per_launch": ms_l,
+             "binding": BINDING.get(name, "unmeasured")}
+        if traffic:
+            r["dram_gbs"] = traffic / (ms_l * 1e-3) / 1e9
+            r["dram_frac"] = r["dram_gbs"] / peak
+        if name == "knn_join_tc":
+            # every node join is one full 128 x 128 x d FP16 Gram tile on tcgen05
+            flops = 2.0 * 128 * 128 * dim * n
+            r["tensor_tflops"] = flops / (ms_l * 1e-3) / 1e12
+            r["tensor_peak_tflops"] = tflops_peak
+            r["tensor_frac"] = r["tensor_tflops"] / tflops_peak
+        return r
+
+    ranked = sorted(stages, key=lambda k: stages[k][0], reverse=True)
+    name = ranked[0]
 
     extra = {}
+    if rank == 0 and not a.skip_prunes:
+        # the configuration's other prunes on one chosen kNN graph, by the stage timers
+        p = capi.knn_params(K, n, dim, ITERS, capi.KNN_CHOSEN)
+        st = capi.State()
+        capi.check(L.tagore_gnn_descent_device(C.byref(p), C.c_void_p(dev.data_ptr()),
+                                               base.ctypes.data_as(C.c_void_p), n, dim,
+                                               C.byref(st.st)))
+        knn_bufs = st.buffers()
+        st.free()
+        for label, itype, thre in (("vamana_1.2", "Vamana", 1.2), ("cagra", "CAGRA", 1.0),
+                                   ("nsg", "NSG", 1.0)):
+            for rep in range(2):
+                s2 = capi.State.alloc(n, dim, K)
+                for i, (nm, _) in enumerate(capi.BUFFERS[:8]):
+                    s2.upload(i, knn_bufs[nm])
+                torch.cuda.synchronize()
+                capi.check(L.tagore_reset_counters())
+                capi.check(L.tagore_set_profiling(1))
+                capi.pruning(s2, FD, itype, topm=TOPM, thre=thre)
+                torch.cuda.synchronize()
+                capi.check(L.tagore_set_profiling(0))
+                st_ = stage_stats(capi)
+                s2.free()
+            extra[f"prune_{label}_ms"] = sum(v[0] for k, v in st_.items() if k.startswith("prune"))
+            extra[f"prune_{label}_stages_ms"] = {k: v[0] for k, v in st_.items()}
+        del knn_bufs
     if not a.skip_recall and rank == 0:
         samp = np.random.default_rng(0).choice(n, min(n, 10_000), replace=False)
+        seeds = [0x5EED + 7 * i for i in range(4)]
+
+        def seeded(rows, ep, half_t):
+            v = [index_recall(rows, ep, base, queries, half_t, seed=sd) for sd in seeds]
+            return float(np.mean(v)), float(np.std(v, ddof=1) / np.sqrt(len(v)))
+
         for label, mode in (("chosen", capi.KNN_CHOSEN), ("plain", capi.KNN_PLAIN)):
             if label == "plain" and a.skip_plain:
                 continue
@@ -295,14 +369,17 @@ def main():
             extra[f"knn_recall10_{label}"] = recall_knn(g, half_t, samp)
             ep = capi.pruning_cfs(st, FD, "path", "dist", topm=TOPM, thre=THRE)
             rows = st.download(0).reshape(n, K)
-            extra[f"index_recall10_{label}"] = index_recall(rows, ep, base, queries, half_t)
-            if label == "chosen":
-                # the opt-in connectivity fix (edges appended; not part of the timed build)
-                extra["connect_edges_added"] = capi.connect(st, ep)
-                rows = st.download(0).reshape(n, K)
-                extra["index_recall10_chosen_connected"] = index_recall(rows, ep, base, queries,
-                                                                        half_t)
+            m, se = seeded(rows, ep, half_t)
+            extra[f"index_recall10_{label}"] = m
+            extra[f"index_recall10_{label}_stderr"] = se
+            # the opt-in connectivity fix (edges appended; not part of the timed build)
+            extra[f"connect_edges_added_{label}"] = capi.connect(st, ep)
+            rows = st.download(0).reshape(n, K)
+            m, se = seeded(rows, ep, half_t)
+            extra[f"index_recall10_{label}_connected"] = m
+            extra[f"index_recall10_{label}_connected_stderr"] = se
             st.free()
+        extra["index_recall_seeds"] = len(seeds)
 
     e2e = None
     if not a.skip_e2e:
@@ -337,11 +414,8 @@ def main():
                 "vectors_per_s": world * n / value,
                 "plain_fp32_s": plain_ms / 1000.0 if plain_ms else None,
                 "chosen_speedup_vs_plain": (plain_ms / ms) if plain_ms else None,
-                "roofline": {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak,
-                             "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                             "peak_source": peak_kind, "traffic": traffic,
-                             "algorithmic_bytes_per_launch": s_bytes / max(1, s_launch),
-                             "ms_per_launch": s_ms / max(1, s_launch)},
+                "roofline": roofline(name),
+                "roofline_next": [roofline(k) for k in ranked[1:3]],
                 "stages_ms_per_step": {k: v[0] / a.steps for k, v in stages.items()},
                 "gpu_launches": launches,
                 "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu}

@@ -425,6 +425,7 @@ __global__ void __launch_bounds__(kThreads, 3)
       const float hr = live ? s.hnrm[st][r] : 0.0f;
       const float lim = live ? s.kth[st][r] - hr : -INFINITY;
       const bool old_row = live && r >= nn;
+      const bool warp_old = __any_sync(kFull, old_row);
       float bd[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
       uint32_t bc[4] = {kInv, kInv, kInv, kInv};
 #pragma unroll
@@ -463,8 +464,10 @@ __global__ void __launch_bounds__(kThreads, 3)
               cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
             }
           }
-          if (old_row) {
-            // (c, r) for the new rows c: value hr - 2g against c's own limit
+          if (warp_old) {
+            // (c, r) for the new rows c: value hr - 2g against c's own limit.
+            // The warp's rows meet c's slots one at a time: only the warp's
+            // best offer per column goes to the shared list.
             const float4 kc = k4p[k4];
             float w4[4];
             fma2_m2(g[4 * k4], g[4 * k4 + 1], hr, hr, w4[0], w4[1]);
@@ -473,7 +476,11 @@ __global__ void __launch_bounds__(kThreads, 3)
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               const uint32_t c = q * 32 + 4 * k4 + j;
-              if (w4[j] < lc[j] && c < cmax && c < kMaxNew)
+              const bool ok = old_row && w4[j] < lc[j] && c < cmax && c < kMaxNew;
+              const uint32_t o = ok ? (uint32_t)(offer_key(w4[j], 0) >> 32) : 0xFFFFFFFFu;
+              const uint32_t best = __reduce_min_sync(kFull, o);
+              const unsigned at = __ballot_sync(kFull, o == best);
+              if (best != 0xFFFFFFFFu && o == best && (at & ((1u << lane) - 1u)) == 0)
                 offer_insert(s.offer[c], T, offer_key(w4[j], r));
             }
           }

@@ -362,14 +362,29 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
       nfresh += __popc(m);
     }
     __syncwarp();
-    for (uint32_t r = lane; r < nfresh; r += 32) {
+    // Each lane scores its fresh rows r, r + 32, ...; at 128 dims two at a
+    // time, sharing the query's loads.
+    const uint32_t step = dim == 128 ? 64u : 32u;
+    for (uint32_t r = lane; r < nfresh; r += step) {
       const uint32_t j = fresh_at[r];
       const uint32_t a = bm.id[topm + j];
-      const float d = row_dist(query, data + (size_t)a * dim, dim);
+      const bool pair = dim == 128 && r + 32 < nfresh;
+      const uint32_t j2 = pair ? fresh_at[r + 32] : j;
+      const uint32_t a2 = bm.id[topm + j2];
+      float d, d2 = 0.0f;
+      if (pair) row_dist128_x2(data + (size_t)a * dim, data + (size_t)a2 * dim, query, d, d2);
+      else d = row_dist(query, data + (size_t)a * dim, dim);
       bm.dis[topm + j] = d;
       if (ring_id) {
         ring_id[(curr + r) % kSelectCand] = a;
         ring_dis[(curr + r) % kSelectCand] = d;
+      }
+      if (pair) {
+        bm.dis[topm + j2] = d2;
+        if (ring_id) {
+          ring_id[(curr + r + 32) % kSelectCand] = a2;
+          ring_dis[(curr + r + 32) % kSelectCand] = d2;
+        }
       }
     }
     curr += nfresh;
@@ -388,17 +403,16 @@ __device__ __noinline__ void warp_sort_mark(uint32_t* cand, float* dis, uint32_t
                  swap_(dis[u], dis[d]);
                  swap_(cand[u], cand[d]);
                });
-  // Two passes: decide from the unmarked ids, then mark.
-  unsigned marks[(kSelectCand + 128 + 31) / 32];
+  // Marks decided from the unmarked ids: chunks from the last to the first,
+  // so a chunk's comparisons read only its own entries and the last entry of
+  // the chunk before it, none of them marked yet.
   const uint32_t chunks = (len + 31) / 32;
-  for (uint32_t c = 0; c < chunks; ++c) {
+  for (uint32_t c = chunks; c-- > 0;) {
     const uint32_t i = c * 32 + lane;
     const bool rep = i >= 1 && i < len && cand[i] == cand[i - 1];
-    marks[c] = __ballot_sync(kFull, rep);
+    __syncwarp();
+    if (rep) cand[i] = kInv;
   }
-  __syncwarp();
-  for (uint32_t c = 0; c < chunks; ++c)
-    if ((marks[c] >> lane) & 1u) cand[c * 32 + lane] = kInv;
   __syncwarp();
 }
 
@@ -467,9 +481,24 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
     }
     if (!__any_sync(kFull, st != 0)) break;
     if (st == 1) {
+      // One step tests the candidate against the next kept neighbour, or at
+      // 128 dims against the next two: it is dropped if any rule fires, so a
+      // second test can only be wasted, never change the outcome.
       const uint32_t q = sel[s];
-      if (q == c) {
+      const bool two = dim == 128 && s + 1 < nsel;
+      const uint32_t q2 = two ? sel[s + 1] : q;
+      if (q == c || q2 == c) {
         st = 0;  // a repeat of a kept neighbour (:1423-1427)
+      } else if (two) {
+        float res, res2;
+        row_dist128_x2(data + (size_t)q * dim, data + (size_t)q2 * dim, data + (size_t)c * dim,
+                       res, res2);
+        rows += 2;
+        if (pruned_by(metric, res, dc, seld[s], thre) ||
+            pruned_by(metric, res2, dc, seld[s + 1], thre))
+          st = 0;
+        else if ((s += 2) == nsel)
+          st = 2;
       } else {
         const float res = row_dist(data + (size_t)q * dim, data + (size_t)c * dim, dim);
         ++rows;

@@ -1,0 +1,98 @@
+"""The GIST-like and Deep-like configurations at their stated sizes.
+
+  * 1,000,000 x 960 GIST-like (512 components, values in [0, 1]), K = 64,
+    12 iterations: the tensor-core kNN build (K-streamed tile), then
+    Pruning_with_CFS('2-hop', 'angle', 0.5) (NSSG at 60 degrees) and DPG, all
+    at degree 32, TOPM 64;
+  * 2,000,000 x 96 Deep-like (unit-normalised, 1,024 components), K = 64,
+    10 iterations: the tensor-core and plain joins at equal recall, then
+    Vamana with alpha 1.2 at degree 32, TOPM 64.
+
+Each prints its times and recall@10 (against brute force over the FP16 base
+on sampled nodes); the smaller-size tests check the same paths against the
+oracle bit for bit.
+"""
+import time
+
+import numpy as np
+import pytest
+
+from tagore_b200 import synth
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+
+def timed(fn):
+    import torch
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    out = fn()
+    torch.cuda.synchronize()
+    return out, time.perf_counter() - t
+
+
+def knn_recall(st, samp, K):
+    import torch
+    n = st.st.n
+    g = st.download(0).reshape(n, K)
+    x = torch.from_numpy(st.download(2).reshape(n, -1)).cuda().float()
+    q = x[samp]
+    d2 = (q * q).sum(1, keepdim=True) + (x * x).sum(1)[None] - 2.0 * (q @ x.T)
+    d2[torch.arange(len(samp)), torch.as_tensor(samp, device=x.device)] = float("inf")
+    truth = torch.topk(d2, 10, largest=False).indices.cpu().numpy()
+    del x, d2
+    return float(np.mean([len(set(g[s, :10].tolist()) & set(truth[i].tolist())) / 10
+                          for i, s in enumerate(samp)]))
+
+
+def rows_ok(rows, n, fd, dense=False):
+    if dense:
+        return rows[:, :fd].max() < n
+    deg = rows[:, 0]
+    assert deg.max() <= fd - 1
+    return all(rows[u, 1:1 + deg[u]].max(initial=0) < n for u in range(0, n, 997))
+
+
+def test_gist_like_1m_x_960(capi):
+    n, K, FD = 1_000_000, 64, 32
+    base, _ = synth.config(2, n=n)
+    samp = np.random.default_rng(3).choice(n, 1000, replace=False)
+    capi.gnn_descent_host(base[:50_000], K, 2).free()  # warm-up
+    st, t_knn = timed(lambda: capi.gnn_descent_host(base, K, 12))
+    r = knn_recall(st, samp, K)
+    bufs = st.buffers()
+    _, t_nssg = timed(lambda: capi.pruning_cfs(st, FD, "2-hop", "angle", topm=64, thre=0.5))
+    rows = st.download(0).reshape(n, K)
+    assert rows_ok(rows, n, FD)
+    st.free()
+    s2 = capi.State.alloc(n, 960, K)
+    for i, (name, _) in enumerate(capi.BUFFERS[:8]):
+        s2.upload(i, bufs[name])
+    _, t_dpg = timed(lambda: capi.pruning(s2, FD, "DPG"))
+    dense = s2.download(0).reshape(-1)[:n * FD].reshape(n, FD)
+    assert rows_ok(dense, n, FD, dense=True)
+    s2.free()
+    print(f"GIST-like 1M x 960, K=64, 12 iterations: kNN {t_knn:.2f} s recall@10 {r:.4f}; "
+          f"NSSG (2-hop/angle 60 deg) {t_nssg:.2f} s; DPG {t_dpg:.2f} s")
+    assert r > 0.95
+
+
+def test_deep_like_2m_x_96(capi):
+    n, K, FD = 2_000_000, 64, 32
+    base, _ = synth.config(3, n=n)
+    samp = np.random.default_rng(11).choice(n, 3000, replace=False)
+    capi.gnn_descent_host(base[:50_000], K, 2).free()  # warm-up
+    res = {}
+    for label, mode in (("chosen", capi.KNN_CHOSEN), ("plain", capi.KNN_PLAIN)):
+        st, t = timed(lambda: capi.gnn_descent_host(base, K, 10, mode=mode))
+        res[label] = (t, knn_recall(st, samp, K))
+        if label == "chosen":
+            _, t_v = timed(lambda: capi.pruning(st, FD, "Vamana", topm=64, thre=1.2))
+            rows = st.download(0).reshape(n, K)
+            assert rows_ok(rows, n, FD)
+        st.free()
+    print(f"Deep-like 2M x 96, K=64, 10 iterations: chosen {res['chosen'][0]:.2f} s recall@10 "
+          f"{res['chosen'][1]:.4f}; plain {res['plain'][0]:.2f} s recall@10 {res['plain'][1]:.4f}; "
+          f"Vamana alpha 1.2 {t_v:.2f} s")
+    assert res["chosen"][1] >= res["plain"][1] - 0.005
+    assert res["plain"][0] > 2.0 * res["chosen"][0]
