@@ -436,32 +436,37 @@ __global__ void __launch_bounds__(kThreads, 3)
       // cut = min(lim, the row's current T-th kept value), refreshed only when
       // a pair is kept; a column takes the insertion branch only below it
       float cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
+      // Every lane runs every iteration of these loops: the TMEM loads and
+      // the offer reductions below are warp-wide, so a row with no column in
+      // a block skips only its own screening, never the loop.
 #pragma unroll 1
       for (uint32_t q = 0; q * 32 < wmax; ++q) {
         float g[32];
         tmem_ld32(tmem + acc * 128 + ((warp * 32u) << 16) + q * 32u, g);
-        if (q * 32 >= cmax) continue;  // no column of this block pairs with row r
+        const bool mine = q * 32 < cmax;  // a column of this block pairs with row r
         const float4* h4 = reinterpret_cast<const float4*>(&s.hnrm[st][q * 32]);
         const float4* k4p = reinterpret_cast<const float4*>(&s.kth[st][q * 32]);
 #pragma unroll
         for (int k4 = 0; k4 < 8; ++k4) {
           const float4 h = h4[k4];
-          float v4[4];
-          fma2_m2(g[4 * k4], g[4 * k4 + 1], h.x, h.y, v4[0], v4[1]);
-          fma2_m2(g[4 * k4 + 2], g[4 * k4 + 3], h.z, h.w, v4[2], v4[3]);
+          if (mine) {
+            float v4[4];
+            fma2_m2(g[4 * k4], g[4 * k4 + 1], h.x, h.y, v4[0], v4[1]);
+            fma2_m2(g[4 * k4 + 2], g[4 * k4 + 3], h.z, h.w, v4[2], v4[3]);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const uint32_t c = q * 32 + 4 * k4 + j;
-            if (v4[j] < cut && c < cmax && c != r) {
-              float v = v4[j];
-              uint32_t vc = c;
+            for (int j = 0; j < 4; ++j) {
+              const uint32_t c = q * 32 + 4 * k4 + j;
+              if (v4[j] < cut && c < cmax && c != r) {
+                float v = v4[j];
+                uint32_t vc = c;
 #pragma unroll
-              for (int t = 0; t < 4; ++t)
-                if (v < bd[t]) {
-                  swap_(v, bd[t]);
-                  swap_(vc, bc[t]);
-                }
-              cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
+                for (int t = 0; t < 4; ++t)
+                  if (v < bd[t]) {
+                    swap_(v, bd[t]);
+                    swap_(vc, bc[t]);
+                  }
+                cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
+              }
             }
           }
           if (warp_old) {
