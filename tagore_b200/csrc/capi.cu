@@ -626,7 +626,8 @@ int tagore_build_index_host(const TagoreKnnParams* p, const float* data, uint32_
 int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_rows,
                        const uint32_t* local_medoids) {
   if (!p || !local_rows || !local_medoids) return fail(TAGORE_EINVAL, "null argument");
-  LargeBuildFn given = [&](const TagoreLargeParams& q, uint32_t, uint32_t cid, const std::vector<uint32_t>& ids,
+  LargeBuildFn given = [&](const TagoreLargeParams& q, uint32_t, uint32_t cid,
+                           const std::vector<uint32_t>& ids, const float*,
                            std::vector<uint32_t>& rows, uint32_t* medoid) -> int {
     if (!local_rows[cid]) return fail(TAGORE_EINVAL, "no local graph for cluster %u", cid);
     rows.assign(local_rows[cid], local_rows[cid] + ids.size() * (size_t)q.k);
@@ -644,19 +645,24 @@ int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int 
   // gpu_construct (src/large_index.cu:130-279) for one cluster: read
   // [u32 n][n x dim f32], kNN graph without rescale, CFS path/dist prune with
   // alpha = thre, rows back to the host with local ids mapped to global ones.
-  LargeBuildFn build = [devices](const TagoreLargeParams& q, uint32_t worker, uint32_t cid,
-                                 const std::vector<uint32_t>& ids, std::vector<uint32_t>& rows,
-                                 uint32_t* medoid) -> int {
-    TG_CUDA(cudaSetDevice((int)devices[worker]));
-    const uint32_t n = (uint32_t)ids.size(), dim = q.dim;
+  // The cluster file [u32 n][n x dim f32] into pinned memory, on the
+  // builder's reader thread.
+  LargeLoadFn load = [](const TagoreLargeParams& q, uint32_t cid, size_t n, float* dst) -> int {
     const std::string path = std::string(q.data_prefix) + std::to_string(cid);
     FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) return fail(TAGORE_EIO, "cannot open cluster file '%s'", path.c_str());
     uint32_t n_file = 0;
-    std::vector<float> x((size_t)n * dim);
-    const bool ok = std::fread(&n_file, 4, 1, f) == 1 && std::fread(x.data(), 4, x.size(), f) == x.size();
+    const size_t cnt = n * q.dim;
+    const bool ok = std::fread(&n_file, 4, 1, f) == 1 && std::fread(dst, 4, cnt, f) == cnt;
     std::fclose(f);
-    if (!ok) return fail(TAGORE_EIO, "'%s' holds fewer than %u vectors", path.c_str(), n);
+    if (!ok) return fail(TAGORE_EIO, "'%s' holds fewer than %zu vectors", path.c_str(), n);
+    return TAGORE_OK;
+  };
+  LargeBuildFn build = [devices](const TagoreLargeParams& q, uint32_t worker, uint32_t cid,
+                                 const std::vector<uint32_t>& ids, const float* x,
+                                 std::vector<uint32_t>& rows, uint32_t* medoid) -> int {
+    TG_CUDA(cudaSetDevice((int)devices[worker]));
+    const uint32_t n = (uint32_t)ids.size(), dim = q.dim;
     TagoreKnnParams kp{};
     kp.k = q.k;
     kp.n = n;
@@ -666,7 +672,7 @@ int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int 
     kp.rescale = 0;
     kp.seed = 0x7A6Eull + cid;
     TagoreKnnState st{};
-    TG_TRY(tagore_gnn_descent_host(&kp, x.data(), n, dim, &st));
+    TG_TRY(tagore_gnn_descent_host(&kp, x, n, dim, &st));
     TagorePruneParams pp{q.k, n, dim, q.final_degree, q.topm, q.thre};
     int rc = tagore_pruning_cfs(&pp, &st, "path", "dist");
     if (rc == TAGORE_OK) {
@@ -683,7 +689,7 @@ int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int 
     }
     return TAGORE_OK;
   };
-  return large_index_run(*p, devices, ndev, build);
+  return large_index_run(*p, devices, ndev, build, load);
 }
 
 }  // extern "C"

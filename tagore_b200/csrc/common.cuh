@@ -244,70 +244,6 @@ __device__ __forceinline__ float dist_pairs_rounds(Load16 load, uint32_t units) 
   return __fadd_rn(x0[0], y0[0]);
 }
 
-// Two 128-dim distances that share operand b, d(a0, b) and d(a1, b), each the
-// tree of dist128_pairs; b's units are loaded once and the three rows' loads
-// are in flight together.
-__device__ __forceinline__ void level2_pair_x2(const uint4* A0, const uint4* A1, const uint4* B,
-                                               int p, float (&x0)[2], float (&y0)[2],
-                                               float (&x1)[2], float (&y1)[2]) {
-  float lx0[4][2], ly0[4][2], lx1[4][2], ly1[4][2];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const uint4 b = __ldg(B + p + 4 * q), a0 = __ldg(A0 + p + 4 * q), a1 = __ldg(A1 + p + 4 * q);
-    lx0[q][0] = ly0[q][0] = lx0[q][1] = ly0[q][1] = 0.0f;
-    lx1[q][0] = ly1[q][0] = lx1[q][1] = ly1[q][1] = 0.0f;
-    pair_acc(a0, b, lx0[q][0], ly0[q][0], lx0[q][1], ly0[q][1]);
-    pair_acc(a1, b, lx1[q][0], ly1[q][0], lx1[q][1], ly1[q][1]);
-  }
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    float ax = lx0[0][h], ay = ly0[0][h], bx = lx0[1][h], by = ly0[1][h];
-    add2(ax, ay, lx0[2][h], ly0[2][h]);
-    add2(bx, by, lx0[3][h], ly0[3][h]);
-    add2(ax, ay, bx, by);
-    x0[h] = ax;
-    y0[h] = ay;
-    float cx = lx1[0][h], cy = ly1[0][h], dx = lx1[1][h], dy = ly1[1][h];
-    add2(cx, cy, lx1[2][h], ly1[2][h]);
-    add2(dx, dy, lx1[3][h], ly1[3][h]);
-    add2(cx, cy, dx, dy);
-    x1[h] = cx;
-    y1[h] = cy;
-  }
-}
-
-__device__ __forceinline__ float tree_top(float (&xa)[2], float (&ya)[2], float (&xb)[2],
-                                          float (&yb)[2], float (&xc)[2], float (&yc)[2],
-                                          float (&xd)[2], float (&yd)[2]) {
-  // level-2 nodes (0,1) in a, (2,3) in b, (4,5) in c, (6,7) in d: level 3
-  // m + m+4, level 4 m + m+2, level 5 0 + 1, as dist128_pairs
-  add2(xa[0], ya[0], xc[0], yc[0]);
-  add2(xa[1], ya[1], xc[1], yc[1]);
-  add2(xb[0], yb[0], xd[0], yd[0]);
-  add2(xb[1], yb[1], xd[1], yd[1]);
-  add2(xa[0], ya[0], xb[0], yb[0]);
-  add2(xa[1], ya[1], xb[1], yb[1]);
-  add2(xa[0], ya[0], xa[1], ya[1]);
-  return __fadd_rn(xa[0], ya[0]);
-}
-
-static __device__ __noinline__ void row_dist128_x2(const __half* __restrict__ a0,
-                                                   const __half* __restrict__ a1,
-                                                   const __half* __restrict__ b, float& d0,
-                                                   float& d1) {
-  const uint4* A0 = reinterpret_cast<const uint4*>(a0);
-  const uint4* A1 = reinterpret_cast<const uint4*>(a1);
-  const uint4* B = reinterpret_cast<const uint4*>(b);
-  float x0a[2], y0a[2], x0b[2], y0b[2], x0c[2], y0c[2], x0d[2], y0d[2];
-  float x1a[2], y1a[2], x1b[2], y1b[2], x1c[2], y1c[2], x1d[2], y1d[2];
-  level2_pair_x2(A0, A1, B, 0, x0a, y0a, x1a, y1a);  // level-2 nodes 0, 1
-  level2_pair_x2(A0, A1, B, 2, x0c, y0c, x1c, y1c);  // 4, 5
-  level2_pair_x2(A0, A1, B, 1, x0b, y0b, x1b, y1b);  // 2, 3
-  level2_pair_x2(A0, A1, B, 3, x0d, y0d, x1d, y1d);  // 6, 7
-  d0 = tree_top(x0a, y0a, x0b, y0b, x0c, y0c, x0d, y0d);
-  d1 = tree_top(x1a, y1a, x1b, y1b, x1c, y1c, x1d, y1d);
-}
-
 __device__ __forceinline__ float row_dist128(const __half* __restrict__ a,
                                              const __half* __restrict__ b) {
   const uint4* A = reinterpret_cast<const uint4*>(a);

@@ -152,16 +152,22 @@ struct KnnStats {
 int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, cudaStream_t s);
 
 // ---- largeIndex (large_index.cpp) ----
-// Builds cluster `cid` (global ids `ids`) into n x K rows [deg, global ids..]
-// and reports its entry point as a global id. `worker` is the builder thread,
-// an index into the device list.
+// Builds cluster `cid` (global ids `ids`, vectors `data` as the load function
+// left them, or null without one) into n x K rows [deg, global ids..] and
+// reports its entry point as a global id. `worker` is the builder thread, an
+// index into the device list.
 using LargeBuildFn = std::function<int(const TagoreLargeParams&, uint32_t worker, uint32_t cid,
-                                       const std::vector<uint32_t>& ids,
+                                       const std::vector<uint32_t>& ids, const float* data,
                                        std::vector<uint32_t>& rows, uint32_t* medoid)>;
+// Reads cluster `cid`'s n vectors (n x dim FP32) into dst, pinned host memory.
+using LargeLoadFn =
+    std::function<int(const TagoreLargeParams&, uint32_t cid, size_t n, float* dst)>;
 // One builder thread per device-list entry, each taking the next cluster in
-// the merger's order; the host merger consumes them in that order.
+// the merger's order; the host merger consumes them in that order. With a
+// load function, each builder reads its next cluster on a reader thread into
+// one of two pinned buffers while the current cluster builds.
 int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int ndev,
-                    const LargeBuildFn& build);
+                    const LargeBuildFn& build, const LargeLoadFn& load = nullptr);
 
 // ---- base preparation (prep.cu) ----
 // FP16 base = raw * factor (as __float2half) and exact FP32 squared norms of

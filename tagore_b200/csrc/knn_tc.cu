@@ -38,7 +38,6 @@ constexpr uint32_t kTmemCols = 128;          // one 128-column accumulator
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s per wait
 constexpr uint32_t kDone = 0xFFFFFFFFu;      // stage node: the producer has finished
 constexpr float kOneMinusEps = 1.0f - 0.000244140625f;  // 1 - 2^-12, the screen's margin
-constexpr uint32_t kMaxNew = 64;             // new rows of a join list (2 x SAMPLE)
 
 struct __align__(1024) Tile {
   uint8_t x[2][kMaxList][128];  // [64-half column block][row][128 B], SW128
@@ -51,9 +50,6 @@ struct __align__(1024) TcSmem {
   float kth[kStages][kMaxList];
   uint32_t pairs[kConsumers * 4];  // kept (row << 16 | column) pairs of the node
   uint32_t warp_pairs[kConsumers / 32];
-  // offers to new rows from old rows: per new row its best 4 (value, column)
-  // keys (the list builder puts at most 2 x 32 new rows first)
-  unsigned long long offer[kMaxNew][4];
   unsigned long long full_bar[kStages];   // rows landed and stage filled
   unsigned long long empty_bar[kStages];  // consumers done with the stage
   unsigned long long mma_bar[2];          // accumulator written
@@ -138,30 +134,6 @@ __device__ __forceinline__ void fma2_m2(float g0, float g1, float h0, float h1, 
       "mov.b64 {%0, %1}, c;}"
       : "=f"(v0), "=f"(v1)
       : "f"(g0), "f"(g1), "f"(h0), "f"(h1), "f"(-2.0f));
-}
-
-// Screened values as unsigned keys in the same order (negative values too),
-// with the column in the low half; kNoOffer is larger than every key.
-constexpr unsigned long long kNoOffer = ~0ull;
-__device__ __forceinline__ unsigned long long offer_key(float v, uint32_t col) {
-  const uint32_t u = __float_as_uint(v);
-  const uint32_t o = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-  return ((unsigned long long)o << 32) | col;
-}
-__device__ __forceinline__ float offer_value(unsigned long long k) {
-  const uint32_t o = (uint32_t)(k >> 32);
-  return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
-}
-// Adds a key to a row's best-T list of offers: every atomicMin keeps the
-// smaller key in its slot and carries the larger one down, so the T slots end
-// up holding the T smallest keys offered, in order, whatever the interleaving.
-__device__ __forceinline__ void offer_insert(unsigned long long* slots, uint32_t T,
-                                             unsigned long long key) {
-  for (uint32_t t = 0; t < T; ++t) {
-    const unsigned long long old = atomicMin(&slots[t], key);
-    if (old == kNoOffer) return;
-    key = old > key ? old : key;
-  }
 }
 
 // Chunk j (4 halves) of row r inside a swizzled tile.
@@ -349,10 +321,6 @@ __global__ void __launch_bounds__(kThreads, 3)
     s.filled = 0;
     s.consumed = 0;
   }
-  if (tid < kMaxNew) {
-#pragma unroll
-    for (int t = 0; t < 4; ++t) s.offer[tid][t] = kNoOffer;
-  }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;");
@@ -414,104 +382,47 @@ __global__ void __launch_bounds__(kThreads, 3)
       // Pair (r, c) may beat row r's k-th entry only if its screened distance
       // nr + nc - 2g is below thr + eps (nr + nc), i.e. hc - 2g < thr - (1-eps) nr
       // with hc = (1-eps) nc (eps = 2^-12). Candidates are ranked by hc - 2g.
-      // Rows are ordered new first. A pair needs at least one new row, and
-      // the tile X X^T is symmetric, so every row reads only the new columns:
-      // a new row screens its pairs with the other new rows itself, and an
-      // old row screens both directions of its pairs with the new rows,
-      // offering (c, r) to new row c through c's shared best-T list. Every
-      // warp then reads the same number of column blocks, where a warp of new
-      // rows used to read all of them while the others waited.
       const bool live = r < total;
-      const float hr = live ? s.hnrm[st][r] : 0.0f;
-      const float lim = live ? s.kth[st][r] - hr : -INFINITY;
-      const bool old_row = live && r >= nn;
-      const bool warp_old = __any_sync(kFull, old_row);
+      const float lim = live ? s.kth[st][r] - s.hnrm[st][r] : -INFINITY;
       float bd[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
       uint32_t bc[4] = {kInv, kInv, kInv, kInv};
 #pragma unroll
       for (int t = 0; t < 4; ++t)
         if ((uint32_t)t >= T) bd[t] = -INFINITY;  // unused slots never accept
-      const uint32_t cmax = live ? nn : 0u;
+      // columns a row may pair with: all others if r is new, new ones if old;
+      // the warp reads only the column blocks one of its rows needs
+      const uint32_t cmax = live ? ((r < nn) ? total : nn) : 0u;
       const uint32_t wmax = __reduce_max_sync(kFull, cmax);
       // cut = min(lim, the row's current T-th kept value), refreshed only when
       // a pair is kept; a column takes the insertion branch only below it
       float cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
-      // Every lane runs every iteration of these loops: the TMEM loads and
-      // the offer reductions below are warp-wide, so a row with no column in
-      // a block skips only its own screening, never the loop.
 #pragma unroll 1
       for (uint32_t q = 0; q * 32 < wmax; ++q) {
         float g[32];
         tmem_ld32(tmem + acc * 128 + ((warp * 32u) << 16) + q * 32u, g);
-        const bool mine = q * 32 < cmax;  // a column of this block pairs with row r
+        if (q * 32 >= cmax) continue;  // no column of this block pairs with row r
         const float4* h4 = reinterpret_cast<const float4*>(&s.hnrm[st][q * 32]);
-        const float4* k4p = reinterpret_cast<const float4*>(&s.kth[st][q * 32]);
 #pragma unroll
         for (int k4 = 0; k4 < 8; ++k4) {
           const float4 h = h4[k4];
-          if (mine) {
-            float v4[4];
-            fma2_m2(g[4 * k4], g[4 * k4 + 1], h.x, h.y, v4[0], v4[1]);
-            fma2_m2(g[4 * k4 + 2], g[4 * k4 + 3], h.z, h.w, v4[2], v4[3]);
+          float v4[4];
+          fma2_m2(g[4 * k4], g[4 * k4 + 1], h.x, h.y, v4[0], v4[1]);
+          fma2_m2(g[4 * k4 + 2], g[4 * k4 + 3], h.z, h.w, v4[2], v4[3]);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const uint32_t c = q * 32 + 4 * k4 + j;
-              if (v4[j] < cut && c < cmax && c != r) {
-                float v = v4[j];
-                uint32_t vc = c;
+          for (int j = 0; j < 4; ++j) {
+            const uint32_t c = q * 32 + 4 * k4 + j;
+            if (v4[j] < cut && c < cmax && c != r) {
+              float v = v4[j];
+              uint32_t vc = c;
 #pragma unroll
-                for (int t = 0; t < 4; ++t)
-                  if (v < bd[t]) {
-                    swap_(v, bd[t]);
-                    swap_(vc, bc[t]);
-                  }
-                cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
-              }
+              for (int t = 0; t < 4; ++t)
+                if (v < bd[t]) {
+                  swap_(v, bd[t]);
+                  swap_(vc, bc[t]);
+                }
+              cut = fminf(lim, T == 1 ? bd[0] : (T == 2 ? bd[1] : (T == 3 ? bd[2] : bd[3])));
             }
           }
-          if (warp_old) {
-            // (c, r) for the new rows c: value hr - 2g against c's own limit.
-            // The warp's rows meet c's slots one at a time: only the warp's
-            // best offer per column goes to the shared list.
-            const float4 kc = k4p[k4];
-            float w4[4];
-            fma2_m2(g[4 * k4], g[4 * k4 + 1], hr, hr, w4[0], w4[1]);
-            fma2_m2(g[4 * k4 + 2], g[4 * k4 + 3], hr, hr, w4[2], w4[3]);
-            const float lc[4] = {kc.x - h.x, kc.y - h.y, kc.z - h.z, kc.w - h.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const uint32_t c = q * 32 + 4 * k4 + j;
-              const bool ok = old_row && w4[j] < lc[j] && c < cmax && c < kMaxNew;
-              const uint32_t o = ok ? (uint32_t)(offer_key(w4[j], 0) >> 32) : 0xFFFFFFFFu;
-              const uint32_t best = __reduce_min_sync(kFull, o);
-              const unsigned at = __ballot_sync(kFull, o == best);
-              if (best != 0xFFFFFFFFu && o == best && (at & ((1u << lane) - 1u)) == 0)
-                offer_insert(s.offer[c], T, offer_key(w4[j], r));
-            }
-          }
-        }
-      }
-      // every consumer has read the accumulator and made its offers: node
-      // i + 1's tile may go in, and the new rows take their offers
-      asm volatile("tcgen05.fence::before_thread_sync;");
-      consumers_sync();
-      if (tid == 0) {
-        const int st1 = (int)((i + 1) % kStages);
-        issue(st1, ph_full[st1], 0u);  // the phase node i + 1 completes
-      }
-      if (live && r < nn && r < kMaxNew) {
-        for (uint32_t t = 0; t < T; ++t) {
-          const unsigned long long k = s.offer[r][t];
-          if (k == kNoOffer) break;
-          s.offer[r][t] = kNoOffer;
-          float v = offer_value(k);
-          uint32_t vc = (uint32_t)(k & 0xFFFFFFFFu);
-#pragma unroll
-          for (int t2 = 0; t2 < 4; ++t2)
-            if (v < bd[t2]) {
-              swap_(v, bd[t2]);
-              swap_(vc, bc[t2]);
-            }
         }
       }
       // kept pairs go to one list so that the exact re-rank is shared evenly
@@ -525,7 +436,13 @@ __global__ void __launch_bounds__(kThreads, 3)
         if (lane >= (uint32_t)o) incl += v;
       }
       if (lane == 31) s.warp_pairs[warp] = incl;
+      // every consumer has read the accumulator: node i + 1's tile may go in
+      asm volatile("tcgen05.fence::before_thread_sync;");
       consumers_sync();
+      if (tid == 0) {
+        const int st1 = (int)((i + 1) % kStages);
+        issue(st1, ph_full[st1], 0u);  // the phase node i + 1 completes
+      }
       uint32_t off = incl - kept, npairs = 0;
 #pragma unroll
       for (int w = 0; w < kConsumers / 32; ++w) {

@@ -301,7 +301,7 @@ int merge_all(const TagoreLargeParams& p, const std::vector<std::vector<uint32_t
 }  // namespace
 
 int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int ndev,
-                    const LargeBuildFn& build) {
+                    const LargeBuildFn& build, const LargeLoadFn& load) {
   if (!p.data_prefix || !p.local_prefix || !p.index_store_path || !p.centers_path)
     return fail(TAGORE_EINVAL, "largeIndex: null path");
   if (ndev < 1 || ndev > 64 || !dev_list)
@@ -358,41 +358,120 @@ int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int nd
     sh.cv.notify_all();
   });
   const uint32_t workers = (uint32_t)ndev;
-  const uint32_t ahead = 2 * workers;  // clusters built but not yet merged
+  const uint32_t ahead = 2 * workers;  // clusters claimed but not yet merged
   uint32_t next = 0;                   // next cluster (merge order) to hand out, under sh.mu
+  size_t largest = 0;
+  for (uint32_t c = 0; c < C; ++c) largest = std::max(largest, clusters[c].size());
+  auto record = [&](int rc) {  // under sh.mu: the first error wins, with its message
+    if (rc != TAGORE_OK && !sh.error) {
+      sh.error = rc;
+      sh.msg = tagore_last_error();
+    }
+  };
+  // The next cluster if the merger window has room now (no wait).
+  auto try_claim = [&](uint32_t* out) -> bool {
+    std::lock_guard<std::mutex> g(sh.mu);
+    if (sh.error || next >= C || sh.consumed + ahead <= next) return false;
+    *out = next++;
+    return true;
+  };
+  auto claim = [&](uint32_t* out) -> bool {
+    std::unique_lock<std::mutex> lk(sh.mu);
+    if (!wait_for(sh, lk, [&] { return next >= C || sh.consumed + ahead > next; })) {
+      if (!sh.error) {
+        sh.error = TAGORE_ETIMEOUT;
+        sh.msg = "largeIndex: merger stalled";
+      }
+      sh.cv.notify_all();
+      return false;
+    }
+    if (sh.error || next >= C) return false;
+    *out = next++;
+    return true;
+  };
+  // A reader thread fills one pinned buffer with a cluster's vectors while
+  // the builder works on the other.
+  struct Prefetch {
+    std::thread t;
+    int rc = TAGORE_OK;
+    std::string msg;
+    void start(const LargeLoadFn& fn, const TagoreLargeParams& q, uint32_t cid, size_t n,
+               float* dst) {
+      rc = TAGORE_OK;
+      msg.clear();
+      t = std::thread([this, &fn, &q, cid, n, dst] {
+        rc = fn(q, cid, n, dst);
+        if (rc != TAGORE_OK) msg = tagore_last_error();
+      });
+    }
+    int wait() {
+      if (t.joinable()) t.join();
+      if (rc != TAGORE_OK) fail(rc, "%s", msg.c_str());
+      return rc;
+    }
+    ~Prefetch() {
+      if (t.joinable()) t.join();
+    }
+  };
   auto builder = [&](uint32_t w) {
-    while (true) {
-      uint32_t i;
-      {
-        std::unique_lock<std::mutex> lk(sh.mu);
-        if (!wait_for(sh, lk, [&] { return next >= C || sh.consumed + ahead > next; })) {
-          if (!sh.error) {
-            sh.error = TAGORE_ETIMEOUT;
-            sh.msg = "largeIndex: merger stalled";
-          }
+    float* pinned[2] = {nullptr, nullptr};
+    struct Free {
+      float** p;
+      ~Free() {
+        for (int b = 0; b < 2; ++b)
+          if (p[b]) cudaFreeHost(p[b]);
+      }
+    } release{pinned};
+    if (load) {
+      const size_t bytes = std::max<size_t>(largest, 1) * q.dim * sizeof(float);
+      for (int b = 0; b < 2; ++b) {
+        count_allocation();
+        if (cudaMallocHost((void**)&pinned[b], bytes) != cudaSuccess) {
+          pinned[b] = nullptr;
+          std::lock_guard<std::mutex> g(sh.mu);
+          record(fail(TAGORE_ENOMEM, "largeIndex: no pinned buffer of %zu bytes", bytes));
           sh.cv.notify_all();
           return;
         }
-        if (sh.error || next >= C) return;
-        i = next++;
       }
+    }
+    uint32_t i = 0;
+    if (!claim(&i)) return;
+    Prefetch pf[2];
+    int buf = 0;
+    if (load) pf[buf].start(load, q, order[i], clusters[order[i]].size(), pinned[buf]);
+    while (true) {
       const uint32_t cid = order[i];
+      int rc = load ? pf[buf].wait() : TAGORE_OK;
+      // the next cluster's file is read while this one builds, when the
+      // merger window already has room for it; otherwise it is claimed
+      // (waiting for the window) after the build, as without a reader
+      uint32_t j = 0;
+      const bool ahead_claimed = rc == TAGORE_OK && load && try_claim(&j);
+      if (ahead_claimed)
+        pf[buf ^ 1].start(load, q, order[j], clusters[order[j]].size(), pinned[buf ^ 1]);
       std::vector<uint32_t> rows;
       uint32_t medoid = 0;
-      const int rc = build(q, w, cid, clusters[cid], rows, &medoid);
-      std::lock_guard<std::mutex> g(sh.mu);
-      if (rc != TAGORE_OK) {
-        if (!sh.error) {
-          sh.error = rc;
-          sh.msg = tagore_last_error();
+      if (rc == TAGORE_OK)
+        rc = build(q, w, cid, clusters[cid], load ? pinned[buf] : nullptr, rows, &medoid);
+      {
+        std::lock_guard<std::mutex> g(sh.mu);
+        if (rc != TAGORE_OK) {
+          record(rc);
+        } else {
+          sh.built[i].rows.swap(rows);
+          sh.built[i].medoid = medoid;
+          sh.built[i].ready = true;
         }
-      } else {
-        sh.built[i].rows.swap(rows);
-        sh.built[i].medoid = medoid;
-        sh.built[i].ready = true;
+        sh.cv.notify_all();
       }
-      sh.cv.notify_all();
       if (rc != TAGORE_OK) return;
+      if (!ahead_claimed) {
+        if (!claim(&j)) return;
+        if (load) pf[buf ^ 1].start(load, q, order[j], clusters[order[j]].size(), pinned[buf ^ 1]);
+      }
+      i = j;
+      buf ^= 1;
     }
   };
   std::vector<std::thread> pool;

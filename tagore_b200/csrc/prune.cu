@@ -362,29 +362,14 @@ __device__ uint32_t warp_beam(const uint32_t* __restrict__ G, const __half* __re
       nfresh += __popc(m);
     }
     __syncwarp();
-    // Each lane scores its fresh rows r, r + 32, ...; at 128 dims two at a
-    // time, sharing the query's loads.
-    const uint32_t step = dim == 128 ? 64u : 32u;
-    for (uint32_t r = lane; r < nfresh; r += step) {
+    for (uint32_t r = lane; r < nfresh; r += 32) {
       const uint32_t j = fresh_at[r];
       const uint32_t a = bm.id[topm + j];
-      const bool pair = dim == 128 && r + 32 < nfresh;
-      const uint32_t j2 = pair ? fresh_at[r + 32] : j;
-      const uint32_t a2 = bm.id[topm + j2];
-      float d, d2 = 0.0f;
-      if (pair) row_dist128_x2(data + (size_t)a * dim, data + (size_t)a2 * dim, query, d, d2);
-      else d = row_dist(query, data + (size_t)a * dim, dim);
+      const float d = row_dist(query, data + (size_t)a * dim, dim);
       bm.dis[topm + j] = d;
       if (ring_id) {
         ring_id[(curr + r) % kSelectCand] = a;
         ring_dis[(curr + r) % kSelectCand] = d;
-      }
-      if (pair) {
-        bm.dis[topm + j2] = d2;
-        if (ring_id) {
-          ring_id[(curr + r + 32) % kSelectCand] = a2;
-          ring_dis[(curr + r + 32) % kSelectCand] = d2;
-        }
       }
     }
     curr += nfresh;
@@ -481,24 +466,9 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
     }
     if (!__any_sync(kFull, st != 0)) break;
     if (st == 1) {
-      // One step tests the candidate against the next kept neighbour, or at
-      // 128 dims against the next two: it is dropped if any rule fires, so a
-      // second test can only be wasted, never change the outcome.
       const uint32_t q = sel[s];
-      const bool two = dim == 128 && s + 1 < nsel;
-      const uint32_t q2 = two ? sel[s + 1] : q;
-      if (q == c || q2 == c) {
+      if (q == c) {
         st = 0;  // a repeat of a kept neighbour (:1423-1427)
-      } else if (two) {
-        float res, res2;
-        row_dist128_x2(data + (size_t)q * dim, data + (size_t)q2 * dim, data + (size_t)c * dim,
-                       res, res2);
-        rows += 2;
-        if (pruned_by(metric, res, dc, seld[s], thre) ||
-            pruned_by(metric, res2, dc, seld[s + 1], thre))
-          st = 0;
-        else if ((s += 2) == nsel)
-          st = 2;
       } else {
         const float res = row_dist(data + (size_t)q * dim, data + (size_t)c * dim, dim);
         ++rows;
