@@ -1,7 +1,9 @@
 #!/bin/sh
 # Compiles the reference Tagore module from its own four .cu files, read in
-# place, for sm_100a into oracle/_ref/ (git-ignored). The result is used only
-# to generate golden fixtures (tests/golden/make_golden.py) on a GPU host.
+# place, for sm_100a into oracle/_ref/ (git-ignored). The module generates
+# golden fixtures (tests/golden/make_golden.py) and runs the interop tests on a
+# GPU host; oracle/_ref/merge_ref runs the reference's largeIndex merger on the
+# CPU (tests/test_large_ref_cpu.py).
 # The reference includes <boost/dynamic_bitset.hpp> for dead CPU code only
 # (src/common.cu:65-148); a small stand-in header is written instead.
 set -e
@@ -31,3 +33,10 @@ SUFFIX=$(python3 -c 'import sysconfig; print(sysconfig.get_config_var("EXT_SUFFI
   "$REF/pybind.cu" "$REF/src/common.cu" "$REF/src/Tagore_src.cu" "$REF/src/large_index.cu" \
   -o "$OUT/Tagore$SUFFIX" -lgomp
 echo "built $OUT/Tagore$SUFFIX"
+# The reference's largeIndex host half (order_merge_main + order_merge_new) on
+# given local graphs, for tests/test_large_ref_cpu.py.
+/usr/local/cuda/bin/nvcc -ccbin /usr/bin/g++ -gencode arch=compute_100a,code=sm_100a -rdc=true -O2 \
+  -std=c++17 -Xcompiler -fopenmp -w -I"$REF/include" -I"$OUT/include" \
+  "$HERE/merge_ref_main.cu" "$REF/src/common.cu" "$REF/src/Tagore_src.cu" "$REF/src/large_index.cu" \
+  -o "$OUT/merge_ref" -lgomp
+echo "built $OUT/merge_ref"
