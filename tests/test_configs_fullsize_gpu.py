@@ -49,7 +49,9 @@ def rows_ok(rows, n, fd, dense=False):
     if dense:
         return rows[:, :fd].max() < n
     deg = rows[:, 0]
-    assert deg.max() <= fd - 1
+    # the select stores at most fd - 1 ids; filter_reverse's union branch up to
+    # fd (src/Tagore_src.cu:1633-1645)
+    assert deg.max() <= fd
     return all(rows[u, 1:1 + deg[u]].max(initial=0) < n for u in range(0, n, 997))
 
 
