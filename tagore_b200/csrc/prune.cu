@@ -1130,6 +1130,8 @@ int run_rank_prune(const Dev& d, const PruneArgs& a, bool dpg, cudaStream_t s) {
   uint32_t* E_tgt = sc.as<uint32_t>();
   uint32_t* E_val = E_tgt + (size_t)d.n * dd;
   const int grid = grid_for(kWarps, d.n);
+  const char* sel_name = dpg ? "prune_select_dpg" : "prune_select_cagra";
+  stage_begin(sel_name, s);
   if (!dpg) {
     const size_t sm = (256 * 4 + (size_t)K * 8) * kWarps;
     TG_TRY(set_smem((const void*)k_select_cagra, sm));
@@ -1140,13 +1142,20 @@ int run_rank_prune(const Dev& d, const PruneArgs& a, bool dpg, cudaStream_t s) {
     k_select_dpg<<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, dd, d.hybrid,
                                                E_tgt, E_val);
   }
+  count_launch();
   TG_CUDA(cudaGetLastError());
+  stage_end(sel_name, s);
+  stage_begin("prune_reverse_store", s);
   TG_TRY(reverse_store(d, E_tgt, E_val, nullptr, dd, 1, cap, dd, s));
+  stage_end("prune_reverse_store", s);
+  stage_begin("prune_filter_reverse_1hop", s);
   const size_t sm2 = ((size_t)dd * 16) * kWarps;
   TG_TRY(set_smem((const void*)k_filter_reverse_1hop, sm2));
   k_filter_reverse_1hop<<<grid, kWarps * 32, sm2, s>>>(d.graph, d.rgraph, d.rnum, d.hybrid, d.n,
                                                        K, dd);
+  count_launch();
   TG_CUDA(cudaGetLastError());
+  stage_end("prune_filter_reverse_1hop", s);
   TG_CUDA(cudaStreamSynchronize(s));
   return TAGORE_OK;
 }
