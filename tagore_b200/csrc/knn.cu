@@ -23,6 +23,8 @@
 #include <algorithm>
 #include <vector>
 
+#include <cub/cub.cuh>
+
 #include "common.cuh"
 #include "internal.h"
 #include "knn_shared.cuh"
@@ -75,7 +77,8 @@ __global__ void __launch_bounds__(128)
 // First S new and first S old entries of each row; new ones become old.
 // Reverse samples are appended to the sampled nodes' lists (capacity S).
 __global__ void __launch_bounds__(128)
-    k_sample(uint64_t* __restrict__ nb, uint32_t n, uint32_t K, uint32_t S,
+    k_sample(uint64_t* __restrict__ nb, const float* __restrict__ norms, float2* __restrict__ meta,
+             uint32_t n, uint32_t K, uint32_t S,
              uint32_t* __restrict__ fnew, uint32_t* __restrict__ fold, uint32_t* __restrict__ fcnt,
              uint32_t* __restrict__ rnew, uint32_t* __restrict__ rold,
              uint32_t* __restrict__ rcnt) {
@@ -97,6 +100,7 @@ __global__ void __launch_bounds__(128)
         row[j] = k & ~1ull;
       }
       if (isold && ro < S) fold[(size_t)u * S + ro] = key_id(k);
+      if (j == K - 1) meta[u] = make_float2(norms[u], kth_of(k));
       cn += __popc(mn);
       co += __popc(mo);
     }
@@ -404,6 +408,34 @@ __global__ void k_finalize(const uint64_t* __restrict__ nb, uint32_t n, uint32_t
   }
 }
 
+// Processing order of the tensor-core joins. A node's join writes only
+// proposals into the pool and reads the rows of its list, so the order in
+// which nodes are taken changes no result. Taking together nodes whose lists
+// overlap keeps the gathered rows resident in L2. Labels: each node takes the
+// smallest label among itself and its first kOrderHops current neighbours,
+// in place (labels only decrease, so concurrent updates are harmless), for
+// kOrderRounds rounds; the order is the nodes sorted by label.
+constexpr uint32_t kOrderHops = 4, kOrderRounds = 16;
+
+__global__ void k_order_init(uint32_t* __restrict__ lab, uint32_t* __restrict__ ids, uint32_t n) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    lab[u] = u;
+    ids[u] = u;
+  }
+}
+
+__global__ void k_order_min(const uint64_t* __restrict__ nb, uint32_t K, uint32_t hops,
+                            uint32_t* lab, uint32_t n) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    uint32_t m = lab[u];
+    for (uint32_t j = 0; j < hops; ++j) {
+      const uint64_t k = __ldg(nb + (size_t)u * K + j);
+      if (k != kEmpty) m = min(m, lab[key_id(k)]);
+    }
+    if (m < lab[u]) lab[u] = m;
+  }
+}
+
 int sm_count() {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -612,6 +644,47 @@ int join_plain(const Work& w, cudaStream_t s) {
   }
 }
 
+// Label bits of n nodes, and the radix sort's scratch for them.
+static int order_bits(uint32_t n) {
+  int end_bit = 1;
+  while (end_bit < 32 && ((uint64_t)1 << end_bit) <= n) ++end_bit;
+  return end_bit;
+}
+static size_t order_sort_bytes(uint32_t n) {
+  size_t tmp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                  (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, 0,
+                                  order_bits(n));
+  return tmp;
+}
+
+// Bytes of scratch order_nodes needs for n nodes.
+size_t order_bytes(uint32_t n) { return (size_t)n * 16 + order_sort_bytes(n) + 256; }
+
+// Writes the join order (see k_order_min) into scratch `buf` of
+// order_bytes(n) bytes and points w.order at it.
+int order_nodes(Work& w, void* buf, cudaStream_t s) {
+  const uint32_t n = w.n, hops = std::min(kOrderHops, w.K);
+  const int end_bit = order_bits(n);
+  uint32_t* lab = static_cast<uint32_t*>(buf);
+  uint32_t* ids = lab + n;
+  uint32_t* lab2 = ids + n;
+  uint32_t* out = lab2 + n;
+  void* tmp_p = reinterpret_cast<char*>(out + n) + (256 - ((uintptr_t)(out + n) & 255)) % 256;
+  size_t tmp = order_sort_bytes(n);
+  const int g = sm_count() * 8;
+  k_order_init<<<g, 256, 0, s>>>(lab, ids, n);
+  count_launch();
+  for (uint32_t r = 0; r < kOrderRounds; ++r) {
+    k_order_min<<<g, 256, 0, s>>>(w.nb, w.K, hops, lab, n);
+    count_launch();
+  }
+  TG_CUDA(cudaGetLastError());
+  TG_CUDA(cub::DeviceRadixSort::SortPairs(tmp_p, tmp, lab, lab2, ids, out, (int)n, 0, end_bit, s));
+  w.order = out;
+  return TAGORE_OK;
+}
+
 }  // namespace knn
 
 // The exact join for a width and mode: the tensor-core tile up to 128 dims,
@@ -646,10 +719,12 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   const size_t nbB = (size_t)d.n * K * 8, poolB = (size_t)d.n * P * 8;
   const size_t listB = (size_t)d.n * S * 4;
   Scratch sc(s);
-  TG_TRY(sc.alloc(nbB + poolB + 4 * listB + (size_t)d.n * kMaxList * 4 + (size_t)d.n * 24 + 256));
+  TG_TRY(sc.alloc(nbB + poolB + 4 * listB + (size_t)d.n * kMaxList * 4 + (size_t)d.n * 32 + 256));
   unsigned char* p = sc.as<unsigned char>();
   w.nb = reinterpret_cast<uint64_t*>(p);
   p += nbB;
+  w.meta = reinterpret_cast<float2*>(p);
+  p += (size_t)d.n * 8;
   w.pool = reinterpret_cast<unsigned long long*>(p);
   p += poolB;
   w.fnew = reinterpret_cast<uint32_t*>(p);
@@ -686,13 +761,24 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   mlp::Net net;
   Scratch zbuf(s);
   ScreenStats sst{};
+  // the tensor-core joins take the nodes in locality order from the second
+  // iteration on (the first one's rows are random), recomputed once more at
+  // the fourth as the rows settle
+  const bool ordered = a.mode != TAGORE_KNN_PLAIN && tc_width;
+  Scratch obuf(s);
+  if (ordered && a.iters > 1) TG_TRY(obuf.alloc(order_bytes(d.n)));
   for (uint32_t it = 0; it < a.iters; ++it) {
+    if (ordered && (it == 1 || it == 3)) {
+      stage_begin("knn_order", s);
+      TG_TRY(order_nodes(w, obuf.as<unsigned char>(), s));
+      stage_end("knn_order", s);
+    }
     TG_CUDA(cudaMemsetAsync(w.rcnt, 0, (size_t)d.n * 8, s));
     stage_begin("knn_sample", s);
-    k_sample<<<sms * 16, 128, 0, s>>>(w.nb, d.n, K, S, w.fnew, w.fold, w.fcnt, w.rnew, w.rold,
+    k_sample<<<sms * 16, 128, 0, s>>>(w.nb, w.norms, w.meta, d.n, K, S, w.fnew, w.fold, w.fcnt, w.rnew, w.rold,
                                        w.rcnt);
     count_launch();
-    stage_end("knn_sample", s, n64 * K * 8 + n64 * 2 * S * 4 * 2, n64);
+    stage_end("knn_sample", s, n64 * K * 8 + n64 * 2 * S * 4 * 2 + n64 * 12, n64);
     TG_CUDA(cudaGetLastError());
     stage_begin("knn_lists", s);
     k_build_lists<<<sms * 16, 128, 0, s>>>(d.n, S, w.fnew, w.fold, w.fcnt, w.rnew, w.rold, w.rcnt,
@@ -768,9 +854,10 @@ int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, 
   TG_CUDA(cudaMemcpyAsync(h, w.stats, sizeof(h), cudaMemcpyDeviceToHost, s));
   TG_CUDA(cudaStreamSynchronize(s));
   if ((uint32_t)h[4] != 0) return fail(TAGORE_ETIMEOUT, "tensor-core join: a bounded wait ran out");
-  // join traffic: each gathered row (FP16 vector, norm, k-th key, list id),
-  // one 8-byte count pair per node, one 8-byte read-modify-write per proposal
-  stage_add(join_name, h[3] * (2ull * d.dim + 16) + n64 * a.iters * 8 + h[0] * 16, h[1]);
+  // join traffic: each gathered row (FP16 vector, 8-byte norm and k-th
+  // distance record, list id), one 8-byte count pair per node, one 8-byte
+  // read-modify-write per proposal
+  stage_add(join_name, h[3] * (2ull * d.dim + 12) + n64 * a.iters * 8 + h[0] * 16, h[1]);
   if (st) {
     st->proposals = h[0];
     st->pairs = h[1];

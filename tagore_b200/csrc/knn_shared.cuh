@@ -25,6 +25,11 @@ struct Work {
   // [0] proposals, [1] exact pairs, [2] row updates, [3] rows gathered, [4] error flag,
   // [5..9] learned-screen measurements (16 slots)
   unsigned long long* stats;
+  // [n] (norm, k-th distance of the row): the tensor-core joins' per-row
+  // screen inputs in one 8-byte record, written by k_sample each iteration
+  float2* meta;
+  // order in which the tensor-core joins take the nodes (null: by id)
+  const uint32_t* order = nullptr;
 };
 
 int join_tc(const Work& w, cudaStream_t s);

@@ -200,13 +200,14 @@ __device__ __forceinline__ bool consumers_any(bool v) {
 
 // Producer warp: walks this block's nodes (blockIdx.x, +gridDim.x, ...),
 // skips those without a join, and fills stage j % kStages with node j: ids,
-// norms and k-th distances by the lanes, rows by TMA tile::gather4. Runs
+// norms and k-th distances (one packed record per row) by the lanes, rows by TMA tile::gather4. Runs
 // kStages nodes ahead of the consumers; ends by publishing kDone.
 template <int D>
-__device__ void join_producer(TcSmem& s, const CUtensorMap& tmap, const uint64_t* __restrict__ nb,
-                              const float* __restrict__ norms, const uint32_t* __restrict__ lists,
+__device__ void join_producer(TcSmem& s, const CUtensorMap& tmap, const float2* __restrict__ meta,
+                              const uint32_t* __restrict__ lists,
                               const uint32_t* __restrict__ lcnt, uint32_t n, uint32_t dim,
-                              uint32_t K, unsigned long long* n_rows) {
+                              uint32_t K, unsigned long long* n_rows,
+                              const uint32_t* __restrict__ order) {
   const uint32_t lane = threadIdx.x & 31u, blocks = (dim + 63) / 64;
   uint32_t next = blockIdx.x;
   uint32_t ph_empty[kStages] = {};
@@ -222,19 +223,20 @@ __device__ void join_producer(TcSmem& s, const CUtensorMap& tmap, const uint64_t
       if (!__shfl_sync(kFull, ok ? 1 : 0, 0)) return;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    // next node with a join: 32 candidates per step, one per lane
+    // next node with a join: 32 positions of the order per step, one per lane
     uint32_t u = kDone, nn = 0, tot = 0;
     while (next < n) {
       const uint32_t c = next + lane * gridDim.x;
+      const uint32_t node = c < n ? (order ? __ldg(order + c) : c) : 0u;
       uint2 cnt = make_uint2(0, 0);
-      if (c < n) cnt = *reinterpret_cast<const uint2*>(lcnt + 2 * (size_t)c);
+      if (c < n) cnt = *reinterpret_cast<const uint2*>(lcnt + 2 * (size_t)node);
       const unsigned ok = __ballot_sync(kFull, c < n && cnt.x > 0 && cnt.y >= 2);
       if (ok) {
         const int w = __ffs(ok) - 1;
-        u = next + (uint32_t)w * gridDim.x;
+        u = __shfl_sync(kFull, node, w);
         nn = __shfl_sync(kFull, cnt.x, w);
         tot = __shfl_sync(kFull, cnt.y, w);
-        next = u + gridDim.x;
+        next += ((uint32_t)w + 1u) * gridDim.x;
         break;
       }
       next += 32u * gridDim.x;
@@ -252,8 +254,9 @@ __device__ void join_producer(TcSmem& s, const CUtensorMap& tmap, const uint64_t
     for (uint32_t t = lane; t < tot; t += 32) {
       const uint32_t id = lists[(size_t)u * kMaxList + t];
       s.ids[st][t] = id;
-      s.hnrm[st][t] = kOneMinusEps * norms[id];
-      s.kth[st][t] = kth_of(nb[(size_t)id * K + K - 1]);
+      const float2 m = __ldg(meta + id);
+      s.hnrm[st][t] = kOneMinusEps * m.x;
+      s.kth[st][t] = m.y;
     }
     __syncwarp();
     const uint32_t groups = (tot + 3) / 4, bar = smem_u32(&s.full_bar[st]);
@@ -292,11 +295,12 @@ __device__ void join_producer(TcSmem& s, const CUtensorMap& tmap, const uint64_t
 // accumulators each (240 against 312 ms for the 1M x 128 build's ten joins).
 template <int D>
 __global__ void __launch_bounds__(kThreads, 3)
-    k_join_tc(const __grid_constant__ CUtensorMap tmap, const uint64_t* __restrict__ nb,
-              const float* __restrict__ norms, const uint32_t* __restrict__ lists,
+    k_join_tc(const __grid_constant__ CUtensorMap tmap, const float2* __restrict__ meta,
+              const uint32_t* __restrict__ lists,
               const uint32_t* __restrict__ lcnt, uint32_t n, uint32_t dim, uint32_t K, uint32_t T,
               uint32_t P, unsigned long long* __restrict__ pool,
-              unsigned long long* __restrict__ stats, int* __restrict__ err) {
+              unsigned long long* __restrict__ stats, int* __restrict__ err,
+              const uint32_t* __restrict__ order) {
   extern __shared__ unsigned char smem_raw[];
   TcSmem& s = *reinterpret_cast<TcSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
@@ -328,7 +332,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   unsigned long long n_pairs = 0, n_props = 0, n_rows = 0;
 
   if (warp == kConsumers / 32) {
-    join_producer<D>(s, tmap, nb, norms, lists, lcnt, n, dim, K, &n_rows);
+    join_producer<D>(s, tmap, meta, lists, lcnt, n, dim, K, &n_rows, order);
   } else {
     uint32_t ph_full[kStages] = {}, ph_mma[2] = {0, 0};
     bool pending[2] = {false, false};  // thread 0: committed MMAs not yet waited for
@@ -529,10 +533,11 @@ struct __align__(1024) WideSmem {
 // Producer warp of the wide join: node metadata into slot j % 2, then the
 // node's column blocks, each into the next ring stage once the MMAs that read
 // it before have completed.
-__device__ void wide_producer(WideSmem& s, const CUtensorMap& tmap, const uint64_t* __restrict__ nb,
-                              const float* __restrict__ norms, const uint32_t* __restrict__ lists,
+__device__ void wide_producer(WideSmem& s, const CUtensorMap& tmap, const float2* __restrict__ meta,
+                              const uint32_t* __restrict__ lists,
                               const uint32_t* __restrict__ lcnt, uint32_t n, uint32_t dim,
-                              uint32_t K, unsigned long long* n_rows) {
+                              uint32_t K, unsigned long long* n_rows,
+                              const uint32_t* __restrict__ order) {
   const uint32_t lane = threadIdx.x & 31u, blocks = (dim + 63) / 64;
   uint32_t next = blockIdx.x, fill = 0;
   uint32_t ph_node[kWideNodes] = {};
@@ -550,15 +555,16 @@ __device__ void wide_producer(WideSmem& s, const CUtensorMap& tmap, const uint64
     uint32_t u = kDone, nn = 0, tot = 0;
     while (next < n) {
       const uint32_t c = next + lane * gridDim.x;
+      const uint32_t node = c < n ? (order ? __ldg(order + c) : c) : 0u;
       uint2 cnt = make_uint2(0, 0);
-      if (c < n) cnt = *reinterpret_cast<const uint2*>(lcnt + 2 * (size_t)c);
+      if (c < n) cnt = *reinterpret_cast<const uint2*>(lcnt + 2 * (size_t)node);
       const unsigned ok = __ballot_sync(kFull, c < n && cnt.x > 0 && cnt.y >= 2);
       if (ok) {
         const int w = __ffs(ok) - 1;
-        u = next + (uint32_t)w * gridDim.x;
+        u = __shfl_sync(kFull, node, w);
         nn = __shfl_sync(kFull, cnt.x, w);
         tot = __shfl_sync(kFull, cnt.y, w);
-        next = u + gridDim.x;
+        next += ((uint32_t)w + 1u) * gridDim.x;
         break;
       }
       next += 32u * gridDim.x;
@@ -566,8 +572,9 @@ __device__ void wide_producer(WideSmem& s, const CUtensorMap& tmap, const uint64
     for (uint32_t t = lane; t < tot; t += 32) {
       const uint32_t id = lists[(size_t)u * kMaxList + t];
       s.ids[ns][t] = id;
-      s.hnrm[ns][t] = kOneMinusEps * norms[id];
-      s.kth[ns][t] = kth_of(nb[(size_t)id * K + K - 1]);
+      const float2 m = __ldg(meta + id);
+      s.hnrm[ns][t] = kOneMinusEps * m.x;
+      s.kth[ns][t] = m.y;
     }
     if (lane == 0) {
       s.node[ns] = u;
@@ -671,11 +678,10 @@ __device__ void wide_mma(WideSmem& s, uint32_t tmem, uint32_t dim) {
 
 __global__ void __launch_bounds__(kWideThreads, 2)
     k_join_tc_wide(const __grid_constant__ CUtensorMap tmap, const __half* __restrict__ data,
-                   const uint64_t* __restrict__ nb, const float* __restrict__ norms,
-                   const uint32_t* __restrict__ lists, const uint32_t* __restrict__ lcnt,
+                   const float2* __restrict__ meta, const uint32_t* __restrict__ lists, const uint32_t* __restrict__ lcnt,
                    uint32_t n, uint32_t dim, uint32_t K, uint32_t T, uint32_t P,
                    unsigned long long* __restrict__ pool, unsigned long long* __restrict__ stats,
-                   int* __restrict__ err) {
+                   int* __restrict__ err, const uint32_t* __restrict__ order) {
   extern __shared__ unsigned char smem_raw[];
   WideSmem& s = *reinterpret_cast<WideSmem*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t tid = threadIdx.x, warp = tid >> 5;
@@ -712,7 +718,7 @@ __global__ void __launch_bounds__(kWideThreads, 2)
   unsigned long long n_pairs = 0, n_props = 0, n_rows = 0;
 
   if (warp == 4) {
-    wide_producer(s, tmap, nb, norms, lists, lcnt, n, dim, K, &n_rows);
+    wide_producer(s, tmap, meta, lists, lcnt, n, dim, K, &n_rows, order);
   } else if (warp == 5) {
     if ((tid & 31u) == 0) wide_mma(s, tmem, dim);
     __syncwarp();
@@ -921,8 +927,8 @@ int launch(const Work& w, const CUtensorMap& map, cudaStream_t s) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int* err = reinterpret_cast<int*>(w.stats + 4);
-  k_join_tc<D><<<sms * 3, kThreads, sm, s>>>(map, w.nb, w.norms, w.lists, w.lcnt, w.n, w.dim,
-                                             w.K, w.T, w.P, w.pool, w.stats, err);
+  k_join_tc<D><<<sms * 3, kThreads, sm, s>>>(map, w.meta, w.lists, w.lcnt, w.n, w.dim,
+                                             w.K, w.T, w.P, w.pool, w.stats, err, w.order);
   TG_CUDA(cudaGetLastError());
   return TAGORE_OK;
 }
@@ -935,8 +941,9 @@ int launch_wide(const Work& w, const CUtensorMap& map, cudaStream_t s) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int* err = reinterpret_cast<int*>(w.stats + 4);
-  k_join_tc_wide<<<sms * 2, kWideThreads, sm, s>>>(map, w.data, w.nb, w.norms, w.lists, w.lcnt,
-                                                    w.n, w.dim, w.K, w.T, w.P, w.pool, w.stats, err);
+  k_join_tc_wide<<<sms * 2, kWideThreads, sm, s>>>(map, w.data, w.meta, w.lists, w.lcnt,
+                                                    w.n, w.dim, w.K, w.T, w.P, w.pool, w.stats, err,
+                                                    w.order);
   TG_CUDA(cudaGetLastError());
   return TAGORE_OK;
 }

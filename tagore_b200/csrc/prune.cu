@@ -514,6 +514,33 @@ struct SelLayout {
 };
 
 // ---------------------------------------------------------------------------
+// Processing order of the select kernels. A node's select reads only the kNN
+// snapshot and writes only its own rows, so the order in which nodes are
+// taken changes no result. Taking together nodes that share kNN
+// neighbourhoods keeps the rows the warps in flight gather resident in L2
+// (at d = 960 the base is 15x larger than L2). Labels: each node takes the
+// smallest label among itself and its first kLabelHops neighbours, in place
+// (labels only decrease, so concurrent updates are harmless), for
+// kLabelRounds rounds; nodes of one cluster converge to a common label. The
+// order is the nodes sorted by label.
+constexpr uint32_t kLabelHops = 4, kLabelRounds = 16;
+
+__global__ void k_label_init(uint32_t* __restrict__ lab, uint32_t* __restrict__ ids, uint32_t n) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    lab[u] = u;
+    ids[u] = u;
+  }
+}
+
+__global__ void k_label_min(const uint32_t* __restrict__ G, uint32_t K, uint32_t hops,
+                            uint32_t* lab, uint32_t n) {
+  for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    uint32_t m = lab[u];
+    for (uint32_t j = 0; j < hops; ++j) m = min(m, lab[__ldg(G + (size_t)u * K + j)]);
+    if (m < lab[u]) lab[u] = m;
+  }
+}
+
 __global__ void k_validate(const uint32_t* __restrict__ g, size_t cnt, uint32_t n,
                            uint32_t* bad) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt;
@@ -545,6 +572,10 @@ __device__ __forceinline__ uint32_t next_node(uint32_t* ctr, int lane) {
   if (lane == 0) b = atomicAdd(ctr, 1u);
   return __shfl_sync(kFull, b, 0);
 }
+// The node at position i of the processing order (identity without one).
+__device__ __forceinline__ uint32_t node_at(const uint32_t* __restrict__ order, uint32_t i) {
+  return order ? __ldg(order + i) : i;
+}
 
 // ring_ids / ring_dis: per-warp rings of kSelectCand scored nodes (path
 // collect), indexed by the warp's global number.
@@ -555,7 +586,7 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
              uint32_t* __restrict__ ctr, uint32_t topm, uint32_t fd, float thre,
              uint32_t* __restrict__ P_ids, float* __restrict__ P_dis, uint32_t* __restrict__ P_cnt,
              unsigned long long* __restrict__ work, uint32_t* __restrict__ ring_ids,
-             float* __restrict__ ring_dis) {
+             float* __restrict__ ring_dis, const uint32_t* __restrict__ order) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   SelLayout lay{kPath ? topm + K : 0u, kSelectCand + K, fd};
@@ -570,7 +601,8 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
   float* rds = kPath ? ring_dis + gw * kSelectCand : nullptr;
   const uint32_t L = lay.L;
   const uint32_t ep = kPath ? *ep_dev : 0u;
-  for (uint32_t b = next_node(ctr, lane); b < n; b = next_node(ctr, lane)) {
+  for (uint32_t pos = next_node(ctr, lane); pos < n; pos = next_node(ctr, lane)) {
+    const uint32_t b = node_at(order, pos);
     const __half* q = data + (size_t)b * dim;
     uint32_t scored = kSelectCand;  // rows scored for this node (2-hop: the 480 collected)
     if (kPath) {
@@ -618,7 +650,8 @@ __global__ void __launch_bounds__(kWarps * 32)
                      const uint32_t* __restrict__ rg, const float* __restrict__ rd,
                      const uint32_t* __restrict__ rnum, const __half* __restrict__ data,
                      uint32_t n, uint32_t dim, uint32_t K, uint32_t fd, int metric, float thre,
-                     const uint32_t* __restrict__ P_ids, const uint32_t* __restrict__ P_cnt) {
+                     const uint32_t* __restrict__ P_ids, const uint32_t* __restrict__ P_cnt,
+                     const uint32_t* __restrict__ order) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t cap = fd + K;  // cur_num <= fd - 1, rever_num <= K
@@ -627,7 +660,8 @@ __global__ void __launch_bounds__(kWarps * 32)
   float* cdis = reinterpret_cast<float*>(cand + cap);
   uint32_t* sel = reinterpret_cast<uint32_t*>(cdis + cap);
   float* seld = reinterpret_cast<float*>(sel + fd);
-  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+  for (uint32_t pos = blockIdx.x * kWarps + warp; pos < n; pos += gridDim.x * kWarps) {
+    const uint32_t b = node_at(order, pos);
     const uint32_t cur_num = P_cnt[b];
     const uint32_t rn = min(K, rnum[b]);
     const uint32_t len = cur_num + rn;
@@ -1041,6 +1075,34 @@ int set_smem(const void* fn, size_t bytes) {
 }
 
 // Select (path or 2-hop) + reverse store + filter_reverse.
+// The select's processing order (see k_label_min), in scratch `sc`.
+int locality_order(const Dev& d, Scratch& sc, const uint32_t** order, cudaStream_t s) {
+  const uint32_t n = d.n, hops = std::min(kLabelHops, d.k);
+  int end_bit = 1;
+  while (end_bit < 32 && ((uint64_t)1 << end_bit) <= n) ++end_bit;
+  size_t tmp = 0;
+  TG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                          (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, 0,
+                                          end_bit, s));
+  TG_TRY(sc.alloc((size_t)n * 16 + tmp + 256));
+  uint32_t* lab = sc.as<uint32_t>();
+  uint32_t* ids = lab + n;
+  uint32_t* lab2 = ids + n;
+  uint32_t* out = lab2 + n;
+  void* tmp_p = reinterpret_cast<char*>(out + n) + (256 - ((uintptr_t)(out + n) & 255)) % 256;
+  const int g = grid_for(256, n);
+  k_label_init<<<g, 256, 0, s>>>(lab, ids, n);
+  count_launch();
+  for (uint32_t r = 0; r < kLabelRounds; ++r) {
+    k_label_min<<<g, 256, 0, s>>>(d.graph, d.k, hops, lab, n);
+    count_launch();
+  }
+  TG_CUDA(cudaGetLastError());
+  TG_CUDA(cub::DeviceRadixSort::SortPairs(tmp_p, tmp, lab, lab2, ids, out, (int)n, 0, end_bit, s));
+  *order = out;
+  return TAGORE_OK;
+}
+
 int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint32_t* ep_host,
                    cudaStream_t s) {
   const uint32_t fd = a.final_degree, K = d.k;
@@ -1078,16 +1140,21 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   uint32_t* ctr = ep_dev + 1;
   TG_CUDA(cudaMemsetAsync(work, 0, 8, s));
   TG_CUDA(cudaMemsetAsync(ctr, 0, sizeof(uint32_t), s));
+  Scratch ord(s);
+  const uint32_t* order = nullptr;
+  stage_begin("prune_order", s);
+  TG_TRY(locality_order(d, ord, &order, s));
+  stage_end("prune_order", s);
   const char* sel_name = path ? "prune_select_path" : "prune_select_2hop";
   stage_begin(sel_name, s);
   if (path)
     k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev, ctr,
                                                  a.topm, fd, a.thre, P_ids, P_dis, P_cnt, work,
-                                                 ring_ids, ring_dis);
+                                                 ring_ids, ring_dis, order);
   else
     k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
                                                   ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt,
-                                                  work, nullptr, nullptr);
+                                                  work, nullptr, nullptr, order);
   count_launch();
   stage_end(sel_name, s);
   TG_CUDA(cudaGetLastError());
@@ -1098,7 +1165,8 @@ int run_dist_prune(const Dev& d, const PruneArgs& a, bool path, int metric, uint
   TG_TRY(set_smem((const void*)k_filter_reverse, sm2));
   stage_begin("prune_filter_reverse", s);
   k_filter_reverse<<<grid, kWarps * 32, sm2, s>>>(d.graph, d.nd, d.rgraph, d.rd, d.rnum, d.data,
-                                                  d.n, d.dim, K, fd, metric, a.thre, P_ids, P_cnt);
+                                                  d.n, d.dim, K, fd, metric, a.thre, P_ids, P_cnt,
+                                                  order);
   count_launch();
   stage_end("prune_filter_reverse", s);
   TG_CUDA(cudaGetLastError());
@@ -1316,11 +1384,11 @@ int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
   if (path)
     k_select<true><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev, ctr,
                                                  a.topm, fd, a.thre, P_ids, P_dis, P_cnt, nullptr,
-                                                 ring_ids, ring_dis);
+                                                 ring_ids, ring_dis, nullptr);
   else
     k_select<false><<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, ep_dev,
                                                   ctr, a.topm, fd, a.thre, P_ids, P_dis, P_cnt,
-                                                  nullptr, nullptr, nullptr);
+                                                  nullptr, nullptr, nullptr, nullptr);
   count_launch();
   TG_CUDA(cudaGetLastError());
 
@@ -1344,7 +1412,8 @@ int prune_cfs_static(const Dev& d, const PruneArgs& a, const std::string& mode,
   const size_t sm2 = ((size_t)(fd + K) * 8 + (size_t)fd * 8 + 16) * kWarps;
   TG_TRY(set_smem((const void*)k_filter_reverse, sm2));
   k_filter_reverse<<<grid, kWarps * 32, sm2, s>>>(d.graph, d.nd, d.rgraph, d.rd, d.rnum, d.data,
-                                                  d.n, d.dim, K, fd, m, a.thre, P_ids, P_cnt);
+                                                  d.n, d.dim, K, fd, m, a.thre, P_ids, P_cnt,
+                                                  nullptr);
   count_launch();
   TG_CUDA(cudaGetLastError());
   if (path && ep_host) TG_CUDA(cudaMemcpyAsync(ep_host, ep_dev, 4, cudaMemcpyDeviceToHost, s));

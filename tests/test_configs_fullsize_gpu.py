@@ -8,10 +8,11 @@
     10 iterations: the tensor-core and plain joins at equal recall, then
     Vamana with alpha 1.2 at degree 32, TOPM 64.
 
-Each prints its times and recall@10 (against brute force over the FP16 base
+Each prints its times (and the GIST-like prunes their stage times) and recall@10 (against brute force over the FP16 base
 on sampled nodes); the smaller-size tests check the same paths against the
 oracle bit for bit.
 """
+import ctypes as C
 import time
 
 import numpy as np
@@ -29,6 +30,21 @@ def timed(fn):
     out = fn()
     torch.cuda.synchronize()
     return out, time.perf_counter() - t
+
+
+def profiled(capi, fn):
+    """fn() under the library's stage timers: (result, seconds, {stage: ms})."""
+    L = capi.lib()
+    capi.check(L.tagore_reset_counters())
+    capi.check(L.tagore_set_profiling(1))
+    try:
+        out, t = timed(fn)
+    finally:
+        capi.check(L.tagore_set_profiling(0))
+    arr = (capi.StageStat * 32)()
+    cnt = C.c_int(0)
+    capi.check(L.tagore_stage_stats(arr, 32, C.byref(cnt)))
+    return out, t, {arr[i].name.decode(): round(arr[i].ms, 1) for i in range(min(cnt.value, 32))}
 
 
 def knn_recall(st, samp, K):
@@ -63,19 +79,20 @@ def test_gist_like_1m_x_960(capi):
     st, t_knn = timed(lambda: capi.gnn_descent_host(base, K, 12))
     r = knn_recall(st, samp, K)
     bufs = st.buffers()
-    _, t_nssg = timed(lambda: capi.pruning_cfs(st, FD, "2-hop", "angle", topm=64, thre=0.5))
+    _, t_nssg, st_nssg = profiled(
+        capi, lambda: capi.pruning_cfs(st, FD, "2-hop", "angle", topm=64, thre=0.5))
     rows = st.download(0).reshape(n, K)
     assert rows_ok(rows, n, FD)
     st.free()
     s2 = capi.State.alloc(n, 960, K)
     for i, (name, _) in enumerate(capi.BUFFERS[:8]):
         s2.upload(i, bufs[name])
-    _, t_dpg = timed(lambda: capi.pruning(s2, FD, "DPG"))
+    _, t_dpg, st_dpg = profiled(capi, lambda: capi.pruning(s2, FD, "DPG"))
     dense = s2.download(0).reshape(-1)[:n * FD].reshape(n, FD)
     assert rows_ok(dense, n, FD, dense=True)
     s2.free()
     print(f"GIST-like 1M x 960, K=64, 12 iterations: kNN {t_knn:.2f} s recall@10 {r:.4f}; "
-          f"NSSG (2-hop/angle 60 deg) {t_nssg:.2f} s; DPG {t_dpg:.2f} s")
+          f"NSSG (2-hop/angle 60 deg) {t_nssg:.2f} s {st_nssg}; DPG {t_dpg:.2f} s {st_dpg}")
     assert r > 0.95
 
 
