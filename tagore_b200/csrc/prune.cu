@@ -501,6 +501,60 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
   return nsel;
 }
 
+// The same filter for rows wider than 128 halves, warp-cooperative. A
+// thread-serial distance over such rows is a long chain of scattered 16-byte
+// loads per lane; here the warp takes the candidates in list order and tests
+// each against the kept neighbours four at a time with coalesced row reads
+// (warp_dist4), stopping at the first group in which a rule fires. A
+// candidate is dropped when any of its tests fires, whichever fires first,
+// so the kept set and the return value are those of warp_filter.
+static __device__ __noinline__ uint32_t warp_filter_wide(const uint32_t* cand, const float* cdis,
+                                                         uint32_t len, uint32_t bid, uint32_t fd,
+                                                         int metric, float thre,
+                                                         const __half* __restrict__ data,
+                                                         uint32_t dim, uint32_t* sel, float* seld,
+                                                         int lane, uint32_t* scored) {
+  uint32_t nsel = 0, last_pos = 0, rows = 0;
+  for (uint32_t i = 0; i < len && nsel < fd; ++i) {
+    const uint32_t c = cand[i];
+    if (c == bid || c == kInv) continue;
+    const float dc = cdis[i];
+    const __half* crow = data + (size_t)c * dim;
+    bool keep = true;
+    for (uint32_t s0 = 0; s0 < nsel && keep; s0 += 4) {
+      uint32_t ids[4];
+      float o[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        ids[t] = s0 + t < nsel ? sel[s0 + t] : kInv;
+        if (ids[t] == c) keep = false;  // a repeat of a kept neighbour (:1423-1427)
+      }
+      if (!keep) break;
+      warp_dist4(crow, data, dim, ids, o, lane);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        if (ids[t] == kInv) continue;
+        ++rows;
+        if (pruned_by(metric, o[t], dc, seld[s0 + t], thre)) keep = false;
+      }
+    }
+    if (keep) {
+      if (lane == 0) {
+        sel[nsel] = c;
+        seld[nsel] = dc;
+      }
+      __syncwarp();
+      ++nsel;
+      last_pos = i;
+    }
+  }
+  __syncwarp();
+  if (scored) *scored = rows;
+  if (nsel == fd) return fd - 1;
+  if (nsel >= 2 && last_pos == len - 1) return nsel - 1;
+  return nsel;
+}
+
 // Per-warp shared layout of the select kernels: the beam (path collect) and
 // the candidate list share one region, since the list is filled only after
 // the beam has finished (its ring of scored nodes lives in global memory).
@@ -616,10 +670,18 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
         cdis[K + i] = in ? rds[i] : kInfDis;
       }
     } else {
-      for (uint32_t i = lane; i < kSelectCand; i += 32) {
-        const uint32_t a = __ldg(G + (size_t)__ldg(G + (size_t)b * K + i / K) * K + i % K);
-        cand[K + i] = a;
-        cdis[K + i] = row_dist(q, data + (size_t)a * dim, dim);
+      for (uint32_t i = lane; i < kSelectCand; i += 32)
+        cand[K + i] = __ldg(G + (size_t)__ldg(G + (size_t)b * K + i / K) * K + i % K);
+      __syncwarp();
+      // The two-hop rows are scored four at a time by the whole warp: each
+      // lane reads its 8-byte chunks of four rows at once (coalesced across
+      // the warp) and the four shuffle trees interleave. Same lane order as
+      // the thread-serial distance, so the same values.
+      for (uint32_t i = 0; i < kSelectCand; i += 4) {
+        const uint32_t ids[4] = {cand[K + i], cand[K + i + 1], cand[K + i + 2], cand[K + i + 3]};
+        float o[4];
+        warp_dist4(q, data, dim, ids, o, lane);
+        if (lane < 4) cdis[K + i + lane] = lane == 0 ? o[0] : lane == 1 ? o[1] : lane == 2 ? o[2] : o[3];
       }
     }
     for (uint32_t i = lane; i < K; i += 32) {
@@ -629,8 +691,11 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
     __syncwarp();
     warp_sort_mark(cand, cdis, L, lane);
     uint32_t filtered = 0;
-    const uint32_t stored = warp_filter(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel,
-                                        seld, lane, &filtered);
+    const uint32_t stored =
+        dim > 128 ? warp_filter_wide(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel,
+                                     seld, lane, &filtered)
+                  : warp_filter(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel, seld,
+                                lane, &filtered);
     if (work && lane == 0) atomicAdd(work, (unsigned long long)(scored + filtered));
     for (uint32_t i = lane; i < stored; i += 32) {
       P_ids[(size_t)b * fd + i] = sel[i];
@@ -678,7 +743,10 @@ __global__ void __launch_bounds__(kWarps * 32)
     uint32_t out_cnt;
     if (len > fd) {
       warp_sort_mark(cand, cdis, len, lane);
-      out_cnt = warp_filter(cand, cdis, len, b, fd, metric, thre, data, dim, sel, seld, lane);
+      out_cnt = dim > 128
+                    ? warp_filter_wide(cand, cdis, len, b, fd, metric, thre, data, dim, sel, seld,
+                                       lane, nullptr)
+                    : warp_filter(cand, cdis, len, b, fd, metric, thre, data, dim, sel, seld, lane);
     } else {
       // Union in ascending reverse-slot order (:1632-1647).
       for (uint32_t i = lane; i < cur_num; i += 32) sel[i] = cand[i];

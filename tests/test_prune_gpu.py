@@ -87,9 +87,17 @@ def test_nsg_k32_final_degree_equals_k_topm_above_k(capi, orc):
     run_pair(capi, orc, case("sift", 3000, 128, 32, seed=2), 32, ("index", "NSG"), topm=64)
 
 
-@pytest.mark.parametrize("itype,thre", [("NSSG", 0.5), ("DPG", 1.0)])
+@pytest.mark.parametrize("itype,thre", [("NSSG", 0.5), ("DPG", 1.0), ("NSG", 1.0), ("Vamana", 1.2)])
 def test_d960(capi, orc, itype, thre):
+    # rows wider than 128 halves take the warp-cooperative filter
     run_pair(capi, orc, case("gist", 1200, 960, 64, seed=3), 32, ("index", itype), thre=thre)
+
+
+@pytest.mark.parametrize("itype,thre", [("NSSG", 0.5), ("Vamana", 1.2)])
+def test_d260_odd_chunks(capi, orc, itype, thre):
+    # 65 four-half chunks: lane 0 of the cooperative tree takes three, the
+    # others two; the thread-serial tree walks 4-half chunks (not 16-byte units)
+    run_pair(capi, orc, case("gist", 900, 260, 48, seed=8), 24, ("index", itype), thre=thre)
 
 
 def test_vamana_d96(capi, orc):
