@@ -555,6 +555,17 @@ static __device__ __noinline__ uint32_t warp_filter_wide(const uint32_t* cand, c
   return nsel;
 }
 
+// Which filter a prune runs. Measured at 1M-2M nodes: the cooperative filter
+// wins wherever the thread-serial tree is not the 128-dim one (d = 96: the
+// Vamana select 1,098 -> 559 ms; d = 960: NSSG 5.5 -> 0.73 s) and, at 128
+// dims, where alpha > 1 keeps long lists that take many tests per candidate
+// (Vamana 1.2: 262 -> 183 ms). At 128 dims with alpha 1 most candidates fall
+// to their first tests, and 32 lanes each working through its own candidate
+// keep more loads in flight (NSG select 203 ms against 254).
+__device__ __forceinline__ bool wide_filter(uint32_t dim, int metric, float thre) {
+  return dim != 128 || (metric == 0 && thre > 1.0f);
+}
+
 // Per-warp shared layout of the select kernels: the beam (path collect) and
 // the candidate list share one region, since the list is filled only after
 // the beam has finished (its ring of scored nodes lives in global memory).
@@ -692,10 +703,11 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
     warp_sort_mark(cand, cdis, L, lane);
     uint32_t filtered = 0;
     const uint32_t stored =
-        dim > 128 ? warp_filter_wide(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel,
-                                     seld, lane, &filtered)
-                  : warp_filter(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel, seld,
-                                lane, &filtered);
+        wide_filter(dim, kPath ? 0 : 1, thre)
+            ? warp_filter_wide(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel, seld,
+                               lane, &filtered)
+            : warp_filter(cand, cdis, L, b, fd, kPath ? 0 : 1, thre, data, dim, sel, seld, lane,
+                          &filtered);
     if (work && lane == 0) atomicAdd(work, (unsigned long long)(scored + filtered));
     for (uint32_t i = lane; i < stored; i += 32) {
       P_ids[(size_t)b * fd + i] = sel[i];
@@ -743,7 +755,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     uint32_t out_cnt;
     if (len > fd) {
       warp_sort_mark(cand, cdis, len, lane);
-      out_cnt = dim > 128
+      out_cnt = wide_filter(dim, metric, thre)
                     ? warp_filter_wide(cand, cdis, len, b, fd, metric, thre, data, dim, sel, seld,
                                        lane, nullptr)
                     : warp_filter(cand, cdis, len, b, fd, metric, thre, data, dim, sel, seld, lane);
