@@ -798,7 +798,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 __global__ void __launch_bounds__(kWarps * 32)
     k_select_cagra(const uint32_t* __restrict__ G, uint32_t n, uint32_t K, uint32_t d,
                    uint32_t* __restrict__ hybrid, uint32_t* __restrict__ E_tgt,
-                   uint32_t* __restrict__ E_val) {
+                   uint32_t* __restrict__ E_val, const uint32_t* __restrict__ order) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr uint32_t H = 256;  // hash slots, K <= 128 keeps the load <= 1/2
@@ -806,7 +806,8 @@ __global__ void __launch_bounds__(kWarps * 32)
   uint32_t* hash = reinterpret_cast<uint32_t*>(mine);
   uint32_t* nei0 = hash + H;
   uint32_t* det = nei0 + K;
-  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+  for (uint32_t pos = blockIdx.x * kWarps + warp; pos < n; pos += gridDim.x * kWarps) {
+    const uint32_t b = node_at(order, pos);
     for (uint32_t j = lane; j < K; j += 32) {
       nei0[j] = __ldg(G + (size_t)b * K + j);
       det[j] = 0;
@@ -867,14 +868,15 @@ __global__ void __launch_bounds__(kWarps * 32)
     k_select_dpg(const uint32_t* __restrict__ G, const float* __restrict__ nd,
                  const __half* __restrict__ data, uint32_t n, uint32_t dim, uint32_t K, uint32_t d,
                  uint32_t* __restrict__ hybrid, uint32_t* __restrict__ E_tgt,
-                 uint32_t* __restrict__ E_val) {
+                 uint32_t* __restrict__ E_val, const uint32_t* __restrict__ order) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned char* mine = smem + (size_t)warp * ((size_t)K * 12);
   uint32_t* nei0 = reinterpret_cast<uint32_t*>(mine);
   uint32_t* det = nei0 + K;
   float* nrow = reinterpret_cast<float*>(det + K);
-  for (uint32_t b = blockIdx.x * kWarps + warp; b < n; b += gridDim.x * kWarps) {
+  for (uint32_t pos = blockIdx.x * kWarps + warp; pos < n; pos += gridDim.x * kWarps) {
+    const uint32_t b = node_at(order, pos);
     for (uint32_t j = lane; j < K; j += 32) {
       nei0[j] = __ldg(G + (size_t)b * K + j);
       det[j] = 0;
@@ -1278,17 +1280,23 @@ int run_rank_prune(const Dev& d, const PruneArgs& a, bool dpg, cudaStream_t s) {
   uint32_t* E_tgt = sc.as<uint32_t>();
   uint32_t* E_val = E_tgt + (size_t)d.n * dd;
   const int grid = grid_for(kWarps, d.n);
+  Scratch ord(s);
+  const uint32_t* order = nullptr;
+  stage_begin("prune_order", s);
+  TG_TRY(locality_order(d, ord, &order, s));
+  stage_end("prune_order", s);
   const char* sel_name = dpg ? "prune_select_dpg" : "prune_select_cagra";
   stage_begin(sel_name, s);
   if (!dpg) {
     const size_t sm = (256 * 4 + (size_t)K * 8) * kWarps;
     TG_TRY(set_smem((const void*)k_select_cagra, sm));
-    k_select_cagra<<<grid, kWarps * 32, sm, s>>>(d.graph, d.n, K, dd, d.hybrid, E_tgt, E_val);
+    k_select_cagra<<<grid, kWarps * 32, sm, s>>>(d.graph, d.n, K, dd, d.hybrid, E_tgt, E_val,
+                                                 order);
   } else {
     const size_t sm = ((size_t)K * 12) * kWarps;
     TG_TRY(set_smem((const void*)k_select_dpg, sm));
     k_select_dpg<<<grid, kWarps * 32, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, dd, d.hybrid,
-                                               E_tgt, E_val);
+                                               E_tgt, E_val, order);
   }
   count_launch();
   TG_CUDA(cudaGetLastError());
