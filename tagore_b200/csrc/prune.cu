@@ -917,6 +917,75 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
 }
 
+// The same select for wide rows, one node per block. The node's K neighbour
+// rows (123 KB at K = 64, d = 960) are read by all K(K-1)/2 pair distances;
+// with one 1,024-thread block per SM they stay in that SM's L1 while its 32
+// warps share the pairs. Work items are (a, m0): row a against the four rows
+// m0..m0+3 (m > a), over the reference's pair set (a < K/2 from the front,
+// a >= K - K/2 from the back, :1715-1717); detour counts are shared-memory
+// integer atomics, so the order of the items changes no count.
+constexpr int kDpgThreads = 1024;
+
+__global__ void __launch_bounds__(kDpgThreads, 1)
+    k_select_dpg_block(const uint32_t* __restrict__ G, const float* __restrict__ nd,
+                       const __half* __restrict__ data, uint32_t n, uint32_t dim, uint32_t K,
+                       uint32_t d, uint32_t* __restrict__ hybrid, uint32_t* __restrict__ E_tgt,
+                       uint32_t* __restrict__ E_val, const uint32_t* __restrict__ order) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int kBlockWarps = kDpgThreads / 32;
+  uint32_t* nei0 = reinterpret_cast<uint32_t*>(smem);
+  uint32_t* det = nei0 + K;
+  float* nrow = reinterpret_cast<float*>(det + K);
+  uint16_t* items = reinterpret_cast<uint16_t*>(nrow + K);  // (a << 8) | m0
+  __shared__ uint32_t n_items;
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (uint32_t a = 0; a + 1 < K; ++a) {
+      if (a >= K / 2 && a < K - K / 2) continue;  // the middle row of an odd K (:1715-1717)
+      for (uint32_t m0 = a + 1; m0 < K; m0 += 4) items[t++] = (uint16_t)((a << 8) | m0);
+    }
+    n_items = t;
+  }
+  __syncthreads();
+  const uint32_t T = n_items;
+  for (uint32_t pos = blockIdx.x; pos < n; pos += gridDim.x) {
+    const uint32_t b = node_at(order, pos);
+    for (uint32_t j = threadIdx.x; j < K; j += kDpgThreads) {
+      nei0[j] = __ldg(G + (size_t)b * K + j);
+      det[j] = 0;
+      nrow[j] = nd[(size_t)b * K + j];
+    }
+    __syncthreads();
+    for (uint32_t t = warp; t < T; t += kBlockWarps) {
+      const uint32_t a = items[t] >> 8, m0 = items[t] & 0xFFu;
+      uint32_t ids[4];
+      float r4[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) ids[q] = (m0 + q < K) ? nei0[m0 + q] : kInv;
+      warp_dist4(data + (size_t)nei0[a] * dim, data, dim, ids, r4, lane);
+      if (lane < 4 && m0 + lane < K) {
+        const float r = lane == 0 ? r4[0] : lane == 1 ? r4[1] : lane == 2 ? r4[2] : r4[3];
+        if (r < nrow[m0 + lane]) atomicAdd(&det[m0 + lane], 1u);
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      warp_network(K, lane, [&](uint32_t u, uint32_t v) { return det[u] > det[v]; },
+                   [&](uint32_t u, uint32_t v) {
+                     swap_(det[u], det[v]);
+                     swap_(nei0[u], nei0[v]);
+                   });
+      for (uint32_t i = lane; i < d; i += 32) {
+        E_tgt[(size_t)b * d + i] = nei0[i];
+        E_val[(size_t)b * d + i] = det[i];
+        hybrid[(size_t)b * K + i] = nei0[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // filter_reverse_1hop (:1812-1886): dense stride-d rows written over the
 // graph buffer (no kernel of this stage reads it), first d/2 forward,
 // then reverse ids by ascending detour that are not already forward, then the
@@ -1292,6 +1361,16 @@ int run_rank_prune(const Dev& d, const PruneArgs& a, bool dpg, cudaStream_t s) {
     TG_TRY(set_smem((const void*)k_select_cagra, sm));
     k_select_cagra<<<grid, kWarps * 32, sm, s>>>(d.graph, d.n, K, dd, d.hybrid, E_tgt, E_val,
                                                  order);
+  } else if (d.dim > 128 && K <= 128) {
+    // the three K-arrays, then the (a, m0) items: fewer than (K/2 + 1)(K/4 + 2) * 2
+    const size_t sm = (size_t)K * 12 + (size_t)(K / 2 + 1) * ((K + 3) / 4 + 1) * 2 * 2 + 16;
+    TG_TRY(set_smem((const void*)k_select_dpg_block, sm));
+    int dev = 0, sms = 148;
+    TG_CUDA(cudaGetDevice(&dev));
+    TG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int g = (int)std::min<uint64_t>(d.n, (uint64_t)sms);
+    k_select_dpg_block<<<g, kDpgThreads, sm, s>>>(d.graph, d.nd, d.data, d.n, d.dim, K, dd,
+                                                  d.hybrid, E_tgt, E_val, order);
   } else {
     const size_t sm = ((size_t)K * 12) * kWarps;
     TG_TRY(set_smem((const void*)k_select_dpg, sm));

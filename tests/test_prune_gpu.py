@@ -93,11 +93,17 @@ def test_d960(capi, orc, itype, thre):
     run_pair(capi, orc, case("gist", 1200, 960, 64, seed=3), 32, ("index", itype), thre=thre)
 
 
-@pytest.mark.parametrize("itype,thre", [("NSSG", 0.5), ("Vamana", 1.2)])
+@pytest.mark.parametrize("itype,thre", [("NSSG", 0.5), ("Vamana", 1.2), ("DPG", 1.0)])
 def test_d260_odd_chunks(capi, orc, itype, thre):
     # 65 four-half chunks: lane 0 of the cooperative tree takes three, the
     # others two; the thread-serial tree walks 4-half chunks (not 16-byte units)
     run_pair(capi, orc, case("gist", 900, 260, 48, seed=8), 24, ("index", itype), thre=thre)
+
+
+def test_dpg_wide_odd_k(capi, orc):
+    # the block-per-node DPG select with an odd K: the reference's pair set
+    # skips the middle row (a = K/2)
+    run_pair(capi, orc, case("gist", 700, 200, 47, seed=9), 24, ("index", "DPG"))
 
 
 def test_vamana_d96(capi, orc):
