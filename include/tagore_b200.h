@@ -130,9 +130,9 @@ int tagore_pruning_cfs_noalloc(const TagorePruneParams* p, TagoreKnnState* st, c
                                const char* metric, void* stream);
 
 /* Tagore.largeIndex(devicelist, DIM, K, cluster_num, max_points, ...)
- * (pybind.cu:298-391). One builder thread per devicelist entry (1 to 64; an id
- * may repeat, which runs that many builders on one device) takes the clusters
- * in the merger's order; the reference deals them round-robin. */
+ * (pybind.cu:298-391). Two builder threads per devicelist entry (1 to 64
+ * entries; an id may repeat, which runs more builders on one device) take the
+ * clusters in the merger's order; the reference deals them round-robin. */
 int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int ndev);
 
 /* The host half of largeIndex alone (reorder + order_merge_new,

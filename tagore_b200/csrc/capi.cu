@@ -627,8 +627,8 @@ int tagore_large_merge(const TagoreLargeParams* p, const uint32_t* const* local_
                        const uint32_t* local_medoids) {
   if (!p || !local_rows || !local_medoids) return fail(TAGORE_EINVAL, "null argument");
   LargeBuildFn given = [&](const TagoreLargeParams& q, uint32_t, uint32_t cid,
-                           const std::vector<uint32_t>& ids, const float*,
-                           std::vector<uint32_t>& rows, uint32_t* medoid) -> int {
+                           const std::vector<uint32_t>& ids, const float*, uint32_t*,
+                           LocalRows& rows, uint32_t* medoid) -> int {
     if (!local_rows[cid]) return fail(TAGORE_EINVAL, "no local graph for cluster %u", cid);
     rows.assign(local_rows[cid], local_rows[cid] + ids.size() * (size_t)q.k);
     *medoid = local_medoids[cid];
@@ -660,7 +660,7 @@ int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int 
   };
   LargeBuildFn build = [devices](const TagoreLargeParams& q, uint32_t worker, uint32_t cid,
                                  const std::vector<uint32_t>& ids, const float* x,
-                                 std::vector<uint32_t>& rows, uint32_t* medoid) -> int {
+                                 uint32_t* stage, LocalRows& rows, uint32_t* medoid) -> int {
     TG_CUDA(cudaSetDevice((int)devices[worker]));
     const uint32_t n = (uint32_t)ids.size(), dim = q.dim;
     TagoreKnnParams kp{};
@@ -675,17 +675,25 @@ int tagore_large_index(const TagoreLargeParams* p, const uint32_t* devices, int 
     TG_TRY(tagore_gnn_descent_host(&kp, x, n, dim, &st));
     TagorePruneParams pp{q.k, n, dim, q.final_degree, q.topm, q.thre};
     int rc = tagore_pruning_cfs(&pp, &st, "path", "dist");
+    // The rows come back in one contiguous copy into the builder's pinned
+    // buffer and are mapped to global ids on their way into the stride-K
+    // rows; a pruned row holds at most min(final_degree, K - 1) ids.
+    const uint32_t W = std::min(q.final_degree, q.k - 1) + 1;
     if (rc == TAGORE_OK) {
-      rows.resize((size_t)n * q.k);
-      cudaError_t e = cudaMemcpy(rows.data(), st.graph, rows.size() * 4, cudaMemcpyDeviceToHost);
+      cudaError_t e = cudaMemcpy(stage, st.graph, (size_t)n * q.k * 4, cudaMemcpyDeviceToHost);
       if (e != cudaSuccess) rc = cuda_fail(e, "cudaMemcpy(cluster rows)", __FILE__, __LINE__);
       *medoid = ids[st.ep];
     }
     tagore_state_free(&st);
     TG_TRY(rc);
+    rows.resize((size_t)n * q.k);
     for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t* src = stage + (size_t)i * q.k;
       uint32_t* r = rows.data() + (size_t)i * q.k;
-      for (uint32_t j = 1; j <= r[0]; ++j) r[j] = ids[r[j]];
+      const uint32_t deg = src[0];
+      if (deg >= W) return fail(TAGORE_ECUDA, "cluster %u row %u holds %u ids (> %u)", cid, i, deg, W - 1);
+      r[0] = deg;
+      for (uint32_t j = 1; j <= deg; ++j) r[j] = ids[src[j]];
     }
     return TAGORE_OK;
   };

@@ -244,6 +244,48 @@ __device__ __forceinline__ float dist_pairs_rounds(Load16 load, uint32_t units) 
   return __fadd_rn(x0[0], y0[0]);
 }
 
+// dist_pairs_rounds with the width fixed at compile time (U 16-byte units),
+// so that every load of the tree is issued up front; the same operations in
+// the same order.
+template <uint32_t U, class Load16>
+__device__ __forceinline__ void level2_pair_fixed(Load16& load, int p, float (&x)[2],
+                                                  float (&y)[2]) {
+  float lx[4][2], ly[4][2];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    lx[q][0] = ly[q][0] = lx[q][1] = ly[q][1] = 0.0f;
+#pragma unroll
+    for (uint32_t u = p + 4 * q; u < U; u += 16)
+      pair_acc(load(u, 0), load(u, 1), lx[q][0], ly[q][0], lx[q][1], ly[q][1]);
+  }
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float ax = lx[0][h], ay = ly[0][h], bx = lx[1][h], by = ly[1][h];
+    add2(ax, ay, lx[2][h], ly[2][h]);
+    add2(bx, by, lx[3][h], ly[3][h]);
+    add2(ax, ay, bx, by);
+    x[h] = ax;
+    y[h] = ay;
+  }
+}
+
+template <uint32_t U, class Load16>
+__device__ __forceinline__ float dist_pairs_fixed(Load16 load) {
+  float x0[2], y0[2], x1[2], y1[2], x2[2], y2[2], x3[2], y3[2];
+  level2_pair_fixed<U>(load, 0, x0, y0);
+  level2_pair_fixed<U>(load, 2, x2, y2);
+  level2_pair_fixed<U>(load, 1, x1, y1);
+  level2_pair_fixed<U>(load, 3, x3, y3);
+  add2(x0[0], y0[0], x2[0], y2[0]);
+  add2(x0[1], y0[1], x2[1], y2[1]);
+  add2(x1[0], y1[0], x3[0], y3[0]);
+  add2(x1[1], y1[1], x3[1], y3[1]);
+  add2(x0[0], y0[0], x1[0], y1[0]);
+  add2(x0[1], y0[1], x1[1], y1[1]);
+  add2(x0[0], y0[0], x0[1], y0[1]);
+  return __fadd_rn(x0[0], y0[0]);
+}
+
 __device__ __forceinline__ float row_dist128(const __half* __restrict__ a,
                                              const __half* __restrict__ b) {
   const uint4* A = reinterpret_cast<const uint4*>(a);
@@ -260,6 +302,11 @@ static __device__ __noinline__ float row_dist(const __half* __restrict__ a,
   const uint2* A = reinterpret_cast<const uint2*>(a);
   const uint2* B = reinterpret_cast<const uint2*>(b);
   if (dim == 128) return row_dist128(a, b);
+  if (dim == 96) {
+    const uint4* A4 = reinterpret_cast<const uint4*>(a);
+    const uint4* B4 = reinterpret_cast<const uint4*>(b);
+    return dist_pairs_fixed<12>([&](uint32_t u, int w) { return __ldg((w ? B4 : A4) + u); });
+  }
   if ((dim & 7u) == 0) {
     const uint4* A4 = reinterpret_cast<const uint4*>(a);
     const uint4* B4 = reinterpret_cast<const uint4*>(b);

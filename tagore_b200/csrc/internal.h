@@ -152,20 +152,42 @@ struct KnnStats {
 int knn_build(const Dev& d, const float* norms, const KnnArgs& a, KnnStats* st, cudaStream_t s);
 
 // ---- largeIndex (large_index.cpp) ----
+// A local graph's rows: n x K, [deg, global ids..]; entries past a row's
+// degree are never read, so resizing leaves them uninitialised.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U>&) {}
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    if constexpr (sizeof...(A) == 0)
+      ::new ((void*)p) U;
+    else
+      ::new ((void*)p) U(std::forward<A>(a)...);
+  }
+};
+using LocalRows = std::vector<uint32_t, NoInitAlloc<uint32_t>>;
 // Builds cluster `cid` (global ids `ids`, vectors `data` as the load function
 // left them, or null without one) into n x K rows [deg, global ids..] and
 // reports its entry point as a global id. `worker` is the builder thread, an
-// index into the device list.
+// index into the device list; `stage` is the builder's pinned buffer of
+// max_points x K words for the rows' way back (null without a load function).
 using LargeBuildFn = std::function<int(const TagoreLargeParams&, uint32_t worker, uint32_t cid,
                                        const std::vector<uint32_t>& ids, const float* data,
-                                       std::vector<uint32_t>& rows, uint32_t* medoid)>;
+                                       uint32_t* stage, LocalRows& rows, uint32_t* medoid)>;
 // Reads cluster `cid`'s n vectors (n x dim FP32) into dst, pinned host memory.
 using LargeLoadFn =
     std::function<int(const TagoreLargeParams&, uint32_t cid, size_t n, float* dst)>;
-// One builder thread per device-list entry, each taking the next cluster in
-// the merger's order; the host merger consumes them in that order. With a
-// load function, each builder reads its next cluster on a reader thread into
-// one of two pinned buffers while the current cluster builds.
+// Builder threads (two per device-list entry with a load function, else one)
+// each take the next cluster in the merger's order; the host merger consumes
+// them in that order. With a load function, each builder reads its next
+// cluster on a reader thread into one of two pinned buffers while the current
+// cluster builds.
 int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int ndev,
                     const LargeBuildFn& build, const LargeLoadFn& load = nullptr);
 

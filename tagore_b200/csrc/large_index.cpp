@@ -6,11 +6,11 @@
 // both are resident, spills evicted local graphs to local_prefix + cid, and
 // finally streams the DiskANN-style index.
 //
-// One builder thread per entry of the device list takes the clusters in the
-// merger's order from a shared counter, so uneven clusters balance over the
-// devices as they come (the reference deals them round-robin,
-// src/large_index.cu:175); the builders run at most two clusters per device
-// ahead of the merger (a host thread). Every wait between them is bounded and
+// Two builder threads per entry of the device list (one when the local
+// graphs are given) take the clusters in the merger's order from a shared
+// counter, so uneven clusters balance over the devices as they come (the
+// reference deals them round-robin, src/large_index.cu:175); the builders run
+// at most two clusters per builder ahead of the merger (a host thread). Every wait between them is bounded and
 // ends in TAGORE_ETIMEOUT. The merged bytes equal a sequential run of the reference's
 // merger (order_merge_new, :286-522) over the same local graphs.
 #include <algorithm>
@@ -103,7 +103,7 @@ void cluster_order(const std::vector<uint32_t>& inter, uint32_t C, uint32_t bs,
 }
 
 struct Built {
-  std::vector<uint32_t> rows;  // n x K, [deg, global ids...]
+  LocalRows rows;  // n x K, [deg, global ids...]
   uint32_t medoid = 0;
   bool ready = false;
 };
@@ -166,7 +166,7 @@ int merge_all(const TagoreLargeParams& p, const std::vector<std::vector<uint32_t
               Shared& sh) {
   const uint32_t C = (uint32_t)clusters.size(), N = p.num, K = p.k, bs = p.buffer_size;
   const uint32_t maxd = p.max_degree;
-  std::vector<std::vector<uint32_t>> pool(bs);
+  std::vector<LocalRows> pool(bs);
   std::vector<uint32_t> buffer(bs, kNone), pointers(N, 0), medoids(C, 0);
   std::vector<uint8_t> visited(N, 0), node_set(N, 0), cached(N, 0);
   std::vector<uint32_t> nhood;
@@ -357,7 +357,11 @@ int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int nd
     if (merge_rc != TAGORE_OK && !sh.error) sh.error = merge_rc;
     sh.cv.notify_all();
   });
-  const uint32_t workers = (uint32_t)ndev;
+  // With a load function (clusters built on devices), two builders share each
+  // device entry: while one copies its rows back and maps them to global
+  // ids, the other's kernels keep the device busy.
+  const uint32_t per_device = load ? 2u : 1u;
+  const uint32_t workers = (uint32_t)ndev * per_device;
   const uint32_t ahead = 2 * workers;  // clusters claimed but not yet merged
   uint32_t next = 0;                   // next cluster (merge order) to hand out, under sh.mu
   size_t largest = 0;
@@ -414,32 +418,37 @@ int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int nd
     }
   };
   auto builder = [&](uint32_t w) {
-    float* pinned[2] = {nullptr, nullptr};
+    // two load buffers (n x dim floats) and the rows' staging buffer
+    void* pinned[3] = {nullptr, nullptr, nullptr};
     struct Free {
-      float** p;
+      void** p;
       ~Free() {
-        for (int b = 0; b < 2; ++b)
+        for (int b = 0; b < 3; ++b)
           if (p[b]) cudaFreeHost(p[b]);
       }
     } release{pinned};
     if (load) {
-      const size_t bytes = std::max<size_t>(largest, 1) * q.dim * sizeof(float);
-      for (int b = 0; b < 2; ++b) {
+      const size_t bytes[3] = {std::max<size_t>(largest, 1) * q.dim * sizeof(float),
+                               std::max<size_t>(largest, 1) * q.dim * sizeof(float),
+                               std::max<size_t>(largest, 1) * q.k * sizeof(uint32_t)};
+      for (int b = 0; b < 3; ++b) {
         count_allocation();
-        if (cudaMallocHost((void**)&pinned[b], bytes) != cudaSuccess) {
+        if (cudaMallocHost(&pinned[b], bytes[b]) != cudaSuccess) {
           pinned[b] = nullptr;
           std::lock_guard<std::mutex> g(sh.mu);
-          record(fail(TAGORE_ENOMEM, "largeIndex: no pinned buffer of %zu bytes", bytes));
+          record(fail(TAGORE_ENOMEM, "largeIndex: no pinned buffer of %zu bytes", bytes[b]));
           sh.cv.notify_all();
           return;
         }
       }
     }
+    float* const bufs[2] = {static_cast<float*>(pinned[0]), static_cast<float*>(pinned[1])};
+    uint32_t* const stage = static_cast<uint32_t*>(pinned[2]);
     uint32_t i = 0;
     if (!claim(&i)) return;
     Prefetch pf[2];
     int buf = 0;
-    if (load) pf[buf].start(load, q, order[i], clusters[order[i]].size(), pinned[buf]);
+    if (load) pf[buf].start(load, q, order[i], clusters[order[i]].size(), bufs[buf]);
     while (true) {
       const uint32_t cid = order[i];
       int rc = load ? pf[buf].wait() : TAGORE_OK;
@@ -449,11 +458,12 @@ int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int nd
       uint32_t j = 0;
       const bool ahead_claimed = rc == TAGORE_OK && load && try_claim(&j);
       if (ahead_claimed)
-        pf[buf ^ 1].start(load, q, order[j], clusters[order[j]].size(), pinned[buf ^ 1]);
-      std::vector<uint32_t> rows;
+        pf[buf ^ 1].start(load, q, order[j], clusters[order[j]].size(), bufs[buf ^ 1]);
+      LocalRows rows;
       uint32_t medoid = 0;
       if (rc == TAGORE_OK)
-        rc = build(q, w, cid, clusters[cid], load ? pinned[buf] : nullptr, rows, &medoid);
+        rc = build(q, w % (uint32_t)ndev, cid, clusters[cid], load ? bufs[buf] : nullptr, stage,
+                   rows, &medoid);
       {
         std::lock_guard<std::mutex> g(sh.mu);
         if (rc != TAGORE_OK) {
@@ -468,7 +478,7 @@ int large_index_run(const TagoreLargeParams& p, const uint32_t* dev_list, int nd
       if (rc != TAGORE_OK) return;
       if (!ahead_claimed) {
         if (!claim(&j)) return;
-        if (load) pf[buf ^ 1].start(load, q, order[j], clusters[order[j]].size(), pinned[buf ^ 1]);
+        if (load) pf[buf ^ 1].start(load, q, order[j], clusters[order[j]].size(), bufs[buf ^ 1]);
       }
       i = j;
       buf ^= 1;
