@@ -9,7 +9,17 @@ and the reverse-edge sort run at full load:
     degree 32, TOPM 64;
   * 1,000,000 x 128 SIFT-like (256 components), K = 96, 10 iterations:
     Pruning_with_CFS('path', 'dist', 1.0), Vamana with alpha 1.2 and CAGRA,
-    all at degree 32, TOPM 64.
+    all at degree 32, TOPM 64;
+  * 500,000 x 96 Deep-like (the 2M configuration's generator), K = 64, 10
+    iterations: Vamana with alpha 1.2 at degree 32 (the cooperative filter and
+    the fixed 96-dim tree);
+  * 200,000 x 960 GIST-like (the 1M configuration's generator), K = 64, 12
+    iterations: NSSG (2-hop collect, angle filter at 60 degrees) and DPG at
+    degree 32 (the cooperative filter and two-hop scoring, the block-per-node
+    DPG select).
+
+The oracle's time at the two larger configurations' own sizes (several
+minutes of CPU each) sets the smaller sizes here; both bases stay above L2.
 
 The kNN graph comes from this library's own GNN_descent; the prune must then
 equal the oracle on every buffer it touches, bit for bit.
@@ -62,6 +72,14 @@ def compare(capi, orc, bufs, n, dim, k, fd, what, topm=64, thre=1.0):
     return rows
 
 
+def knn_buffers_config(capi, cfg, n, k, iters):
+    base, _ = synth.config(cfg, n=n)
+    st = capi.gnn_descent_host(base, k, iters)
+    bufs = st.buffers()
+    st.free()
+    return bufs
+
+
 @pytest.fixture(scope="module")
 def knn_1m(capi):
     return knn_buffers(capi, 1_000_000, 128, 96, 10, 256, 0x7A6E + 1)
@@ -85,3 +103,26 @@ def test_config2_vamana_1m(capi, orc, knn_1m):
 def test_config2_cagra_1m(capi, orc, knn_1m):
     rows = compare(capi, orc, knn_1m, 1_000_000, 128, 96, 32, ("index", "CAGRA"))
     assert rows.shape == (1_000_000, 96)
+
+
+@pytest.fixture(scope="module")
+def knn_deep_500k(capi):
+    return knn_buffers_config(capi, 3, 500_000, 64, 10)
+
+
+def test_config4_vamana_500k_x_96(capi, orc, knn_deep_500k):
+    rows = compare(capi, orc, knn_deep_500k, 500_000, 96, 64, 32, ("index", "Vamana"), thre=1.2)
+    assert rows[:, 0].max() <= 32
+
+
+@pytest.fixture(scope="module")
+def knn_gist_200k(capi):
+    return knn_buffers_config(capi, 2, 200_000, 64, 12)
+
+
+def test_config3_nssg_200k_x_960(capi, orc, knn_gist_200k):
+    compare(capi, orc, knn_gist_200k, 200_000, 960, 64, 32, ("index", "NSSG"), thre=0.5)
+
+
+def test_config3_dpg_200k_x_960(capi, orc, knn_gist_200k):
+    compare(capi, orc, knn_gist_200k, 200_000, 960, 64, 32, ("index", "DPG"))
