@@ -112,6 +112,53 @@ __device__ __forceinline__ void warp_dist4(const __half* __restrict__ q, const _
   for (int t = 0; t < 4; ++t) out[t] = __shfl_sync(kFull, __fadd_rn(x[t], y[t]), 0);
 }
 
+// Eight independent distances against one query at 96 dims, four per
+// half-warp. At 96 dims the reference's lane slots 0..23 hold one 4-half
+// chunk each and slots 24..31 none, so its first tree level (offset 16)
+// adds chunk l + 16 into slot l for l < 8 and adds nothing (an exact + 0) for
+// l = 8..15. Lane l of each half computes slot l's leaf and, for l < 8, slot
+// l + 16's leaf and their level-1 sum itself; levels 2-5 (offsets 8..1) run
+// on shuffles within the half. Same operations in the same order as the
+// full-warp tree, so the same values. Rows with id kInv yield 0 and must be
+// ignored by the caller.
+__device__ __forceinline__ void warp_dist8_d96(const __half* __restrict__ q,
+                                               const __half* __restrict__ base,
+                                               const uint32_t ids[8], float out[8], int lane) {
+  constexpr uint32_t kDim = 96;
+  const int half = lane >> 4, l = lane & 15;
+  const uint2* Q = reinterpret_cast<const uint2*>(q);
+  const uint2 q0 = Q[l];
+  const uint2 q1 = l < 8 ? Q[l + 16] : make_uint2(0u, 0u);
+  float x[4], y[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const uint32_t id = half ? ids[4 + t] : ids[t];
+    x[t] = y[t] = 0.0f;
+    if (id != kInv) {
+      const uint2* R = reinterpret_cast<const uint2*>(base + (size_t)id * kDim);
+      chunk_acc(q0, __ldg(R + l), x[t], y[t]);
+      if (l < 8) {
+        float x1 = 0.0f, y1 = 0.0f;
+        chunk_acc(q1, __ldg(R + l + 16), x1, y1);
+        add2(x[t], y[t], x1, y1);
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 8; off > 0; off >>= 1) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+      add2(x[t], y[t], __shfl_down_sync(kFull, x[t], off, 16),
+           __shfl_down_sync(kFull, y[t], off, 16));
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const float r = __fadd_rn(x[t], y[t]);
+    out[t] = __shfl_sync(kFull, r, 0);
+    out[4 + t] = __shfl_sync(kFull, r, 16);
+  }
+}
+
 // The reference's shuffle-down tree evaluated by one thread over the 32 lane
 // slots: v_L[l] = v_{L-1}[l] + v_{L-1}[l + (32 >> L)], root v_5[0]. Walking
 // the tree depth-first visits the slots in bit-reversed order and keeps at

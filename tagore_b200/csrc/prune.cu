@@ -508,12 +508,15 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
 // (warp_dist4), stopping at the first group in which a rule fires. A
 // candidate is dropped when any of its tests fires, whichever fires first,
 // so the kept set and the return value are those of warp_filter.
-static __device__ __noinline__ uint32_t warp_filter_wide(const uint32_t* cand, const float* cdis,
-                                                         uint32_t len, uint32_t bid, uint32_t fd,
-                                                         int metric, float thre,
-                                                         const __half* __restrict__ data,
-                                                         uint32_t dim, uint32_t* sel, float* seld,
-                                                         int lane, uint32_t* scored) {
+// G kept neighbours per step: 8 at 96 dims (warp_dist8_d96, a half-warp per
+// distance), 4 otherwise (warp_dist4).
+template <int G>
+static __device__ __noinline__ uint32_t warp_filter_group(const uint32_t* cand, const float* cdis,
+                                                          uint32_t len, uint32_t bid, uint32_t fd,
+                                                          int metric, float thre,
+                                                          const __half* __restrict__ data,
+                                                          uint32_t dim, uint32_t* sel, float* seld,
+                                                          int lane, uint32_t* scored) {
   uint32_t nsel = 0, last_pos = 0, rows = 0;
   for (uint32_t i = 0; i < len && nsel < fd; ++i) {
     const uint32_t c = cand[i];
@@ -521,18 +524,21 @@ static __device__ __noinline__ uint32_t warp_filter_wide(const uint32_t* cand, c
     const float dc = cdis[i];
     const __half* crow = data + (size_t)c * dim;
     bool keep = true;
-    for (uint32_t s0 = 0; s0 < nsel && keep; s0 += 4) {
-      uint32_t ids[4];
-      float o[4];
+    for (uint32_t s0 = 0; s0 < nsel && keep; s0 += G) {
+      uint32_t ids[G];
+      float o[G];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
+      for (int t = 0; t < G; ++t) {
         ids[t] = s0 + t < nsel ? sel[s0 + t] : kInv;
         if (ids[t] == c) keep = false;  // a repeat of a kept neighbour (:1423-1427)
       }
       if (!keep) break;
-      warp_dist4(crow, data, dim, ids, o, lane);
+      if constexpr (G == 8)
+        warp_dist8_d96(crow, data, ids, o, lane);
+      else
+        warp_dist4(crow, data, dim, ids, o, lane);
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
+      for (int t = 0; t < G; ++t) {
         if (ids[t] == kInv) continue;
         ++rows;
         if (pruned_by(metric, o[t], dc, seld[s0 + t], thre)) keep = false;
@@ -564,6 +570,18 @@ static __device__ __noinline__ uint32_t warp_filter_wide(const uint32_t* cand, c
 // keep more loads in flight (NSG select 203 ms against 254).
 __device__ __forceinline__ bool wide_filter(uint32_t dim, int metric, float thre) {
   return dim != 128 || (metric == 0 && thre > 1.0f);
+}
+
+static __device__ __forceinline__ uint32_t warp_filter_wide(const uint32_t* cand, const float* cdis,
+                                                            uint32_t len, uint32_t bid, uint32_t fd,
+                                                            int metric, float thre,
+                                                            const __half* __restrict__ data,
+                                                            uint32_t dim, uint32_t* sel, float* seld,
+                                                            int lane, uint32_t* scored) {
+  return dim == 96 ? warp_filter_group<8>(cand, cdis, len, bid, fd, metric, thre, data, dim, sel,
+                                          seld, lane, scored)
+                   : warp_filter_group<4>(cand, cdis, len, bid, fd, metric, thre, data, dim, sel,
+                                          seld, lane, scored);
 }
 
 // Per-warp shared layout of the select kernels: the beam (path collect) and
