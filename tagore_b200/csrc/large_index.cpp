@@ -145,11 +145,15 @@ struct Writer {
 struct Reader {
   FILE* f = nullptr;
   std::vector<char> buf;
-  bool open(const std::string& p) {
+  bool open(const std::string& p, size_t buffer = 1u << 20, uint64_t at = 0) {
     f = std::fopen(p.c_str(), "rb");
     if (f) {
-      buf.resize(1u << 20);
+      buf.resize(buffer);
       std::setvbuf(f, buf.data(), _IOFBF, buf.size());
+      if (at && std::fseek(f, (long)at, SEEK_SET) != 0) {
+        std::fclose(f);
+        f = nullptr;
+      }
     }
     return f != nullptr;
   }
@@ -170,6 +174,13 @@ int merge_all(const TagoreLargeParams& p, const std::vector<std::vector<uint32_t
   std::vector<uint32_t> buffer(bs, kNone), pointers(N, 0), medoids(C, 0);
   std::vector<uint8_t> visited(N, 0), node_set(N, 0), cached(N, 0);
   std::vector<uint32_t> nhood;
+  // The final pass runs over point ranges [lo(r), lo(r + 1)) in parallel;
+  // spill() records where each range starts in each local index file
+  // (members are in ascending global id).
+  const uint32_t R = std::max(1u, std::min({16u, std::thread::hardware_concurrency(),
+                                            N / 4096u + 1u}));
+  auto lo = [&](uint32_t r) { return (uint32_t)((uint64_t)r * N / R); };
+  std::vector<uint64_t> part_off((size_t)C * (R + 1), 0);
   auto take = [&](uint32_t i) -> int {
     std::unique_lock<std::mutex> lk(sh.mu);
     if (!wait_for(sh, lk, [&] { return sh.built[i].ready; }))
@@ -185,13 +196,19 @@ int merge_all(const TagoreLargeParams& p, const std::vector<std::vector<uint32_t
   auto spill = [&](uint32_t cid) -> int {
     Writer w(std::string(p.local_prefix) + std::to_string(cid));
     if (!w.f) return fail(TAGORE_EIO, "cannot create local index for cluster %u", cid);
+    uint64_t* offs = part_off.data() + (size_t)cid * (R + 1);
+    uint64_t at = 0;
+    uint32_t part = 0;
     for (uint32_t j = 0; j < clusters[cid].size(); ++j) {
       const uint32_t* r = row(cid, j);
+      while (part < R && clusters[cid][j] >= lo(part)) offs[part++] = at;
       if (!w.put(r, 4) || !w.put(r + 1, 4ull * r[0]))
         return fail(TAGORE_EIO, "write of local index %u failed", cid);
+      at += 4ull * (1 + r[0]);
       visited[clusters[cid][j]] = 1;
       pointers[clusters[cid][j]] = kNone;
     }
+    while (part <= R) offs[part++] = at;
     if (!w.close()) return fail(TAGORE_EIO, "write of local index %u failed", cid);
     return TAGORE_OK;
   };
@@ -245,51 +262,95 @@ int merge_all(const TagoreLargeParams& p, const std::vector<std::vector<uint32_t
     if (buffer[s] != kNone) TG_TRY(spill(buffer[s]));
   pool.clear();
 
-  // Final merge into the index file (:447-520).
+  // Final merge into the index file (:447-520). Point i's record comes
+  // from the local indexes of its two clusters, read in member order; each
+  // range of points is merged by its own thread from its own file positions
+  // into its own buffer, and the buffers are written in order.
+  std::vector<std::vector<uint32_t>> part_out(R);
+  std::vector<int> part_rc(R, TAGORE_OK);
+  std::vector<std::string> part_msg(R);  // the library's error text is per thread
+  auto final_part = [&](uint32_t r) {
+    std::vector<Reader> shard(C);
+    std::vector<uint8_t> mark(N, 0);
+    std::vector<uint32_t> a(K), b(K), nh;
+    std::vector<uint32_t>& o = part_out[r];
+    auto reader = [&](uint32_t c) -> Reader* {
+      if (!shard[c].f &&
+          !shard[c].open(std::string(p.local_prefix) + std::to_string(c), 64u << 10,
+                         part_off[(size_t)c * (R + 1) + r]))
+        return nullptr;
+      return &shard[c];
+    };
+    for (uint32_t i = lo(r); i < lo(r + 1); ++i) {
+      Reader* f1 = reader(centers[i]);
+      Reader* f2 = reader(second[i]);
+      if (!f1 || !f2) {
+        part_rc[r] = fail(TAGORE_EIO, "cannot open local index of cluster %u",
+                          f1 ? second[i] : centers[i]);
+        part_msg[r] = tagore_last_error();
+        return;
+      }
+      uint32_t d1 = 0, d2 = 0;
+      bool ok;
+      if (cached[i]) {
+        Reader* src = f1;
+        ok = f1->get(&d1, 4);
+        if (ok && d1 == 0) {
+          src = f2;
+          ok = f2->get(&d1, 4);
+        } else if (ok) {
+          ok = f2->get(&d2, 4);
+        }
+        ok = ok && d1 <= K && src->get(a.data(), 4ull * d1);
+        if (ok) {
+          o.push_back(d1);
+          o.insert(o.end(), a.begin(), a.begin() + d1);
+        }
+      } else {
+        ok = f1->get(&d1, 4) && d1 <= K && f1->get(a.data(), 4ull * d1) && f2->get(&d2, 4) &&
+             d2 <= K && f2->get(b.data(), 4ull * d2);
+        if (ok) {
+          nh.clear();
+          for (uint32_t j = 0; j < d1; ++j) {
+            mark[a[j]] = 1;
+            nh.push_back(a[j]);
+          }
+          for (uint32_t j = 0; j < d2; ++j)
+            if (!mark[b[j]]) {
+              mark[b[j]] = 1;
+              nh.push_back(b[j]);
+            }
+          for (uint32_t v : nh) mark[v] = 0;
+          const uint32_t deg = std::min<uint32_t>((uint32_t)nh.size(), maxd);
+          o.push_back(deg);
+          o.insert(o.end(), nh.begin(), nh.begin() + deg);
+        }
+      }
+      if (!ok) {
+        part_rc[r] = fail(TAGORE_EIO, "reading the local indexes failed (point %u)", i);
+        part_msg[r] = tagore_last_error();
+        return;
+      }
+    }
+  };
+  {
+    std::vector<std::thread> th;
+    for (uint32_t r = 1; r < R; ++r) th.emplace_back(final_part, r);
+    final_part(0);
+    for (auto& t : th) t.join();
+  }
+  for (uint32_t r = 0; r < R; ++r)
+    if (part_rc[r] != TAGORE_OK) return fail(part_rc[r], "%s", part_msg[r].c_str());
   Writer out(p.index_store_path);
   if (!out.f) return fail(TAGORE_EIO, "cannot create '%s'", p.index_store_path);
   uint64_t index_size = 0;
   bool ok = out.put(&index_size, 8) && out.put(&maxd, 4) && out.put(&maxd, 4) && out.put(&index_size, 8);
-  std::vector<Reader> shard(C);
-  for (uint32_t c = 0; c < C; ++c)
-    if (!shard[c].open(std::string(p.local_prefix) + std::to_string(c)))
-      return fail(TAGORE_EIO, "cannot open local index of cluster %u", c);
-  std::vector<uint32_t> a(K), b(K);
-  for (uint32_t i = 0; ok && i < N; ++i) {
-    uint32_t d1 = 0, d2 = 0;
-    if (cached[i]) {
-      uint32_t cid = centers[i];
-      ok = shard[cid].get(&d1, 4);
-      if (ok && d1 == 0) {
-        cid = second[i];
-        ok = shard[cid].get(&d1, 4);
-      } else if (ok) {
-        ok = shard[second[i]].get(&d2, 4);
-      }
-      if (d1 > K) return fail(TAGORE_EIO, "corrupt local index record");
-      ok = ok && shard[cid].get(a.data(), 4ull * d1) && out.put(&d1, 4) && out.put(a.data(), 4ull * d1);
-      index_size += 4ull * (1 + d1);
-    } else {
-      ok = shard[centers[i]].get(&d1, 4) && d1 <= K && shard[centers[i]].get(a.data(), 4ull * d1) &&
-           shard[second[i]].get(&d2, 4) && d2 <= K && shard[second[i]].get(b.data(), 4ull * d2);
-      if (!ok) break;
-      nhood.clear();
-      for (uint32_t j = 0; j < d1; ++j) {
-        node_set[a[j]] = 1;
-        nhood.push_back(a[j]);
-      }
-      for (uint32_t j = 0; j < d2; ++j)
-        if (!node_set[b[j]]) {
-          node_set[b[j]] = 1;
-          nhood.push_back(b[j]);
-        }
-      for (uint32_t v : nhood) node_set[v] = 0;
-      const uint32_t deg = std::min<uint32_t>((uint32_t)nhood.size(), maxd);
-      ok = out.put(&deg, 4) && out.put(nhood.data(), 4ull * deg);
-      index_size += 4ull * (1 + deg);
-    }
+  for (uint32_t r = 0; ok && r < R; ++r) {
+    ok = out.put(part_out[r].data(), part_out[r].size() * 4);
+    index_size += part_out[r].size() * 4ull;
+    std::vector<uint32_t>().swap(part_out[r]);
   }
-  if (!ok) return fail(TAGORE_EIO, "reading local indexes or writing '%s' failed", p.index_store_path);
+  if (!ok) return fail(TAGORE_EIO, "writing '%s' failed", p.index_store_path);
   index_size += 24;
   // header: size, max degree, medoid of the last cluster built (:516-519)
   if (std::fflush(out.f) != 0 || std::fseek(out.f, 0, SEEK_SET) != 0 || !out.put(&index_size, 8) ||

@@ -49,7 +49,10 @@ def scenario(seed, N, Cn, K, maxd):
 
 @pytest.mark.parametrize("seed,N,Cn,K,bs,maxd",
                          [(1, 3000, 7, 16, 2, 10), (2, 4000, 9, 24, 3, 12), (3, 2500, 6, 16, 6, 15),
-                          (4, 5000, 12, 32, 4, 22)])
+                          (4, 5000, 12, 32, 4, 22),
+                          # the final pass splits the points into ranges of at least 4,096,
+                          # merged on separate threads: several ranges here
+                          (5, 40000, 16, 24, 5, 16)])
 def test_merge_equals_reference_merger(capi, tmp_path, seed, N, Cn, K, bs, maxd):
     first, second, clusters, rows, eps = scenario(seed, N, Cn, K, maxd)
     ref_dir, our_dir = tmp_path / "ref", tmp_path / "ours"
