@@ -823,7 +823,12 @@ __global__ void __launch_bounds__(kWideThreads, 2)
           const uint4* A4 = reinterpret_cast<const uint4*>(data + (size_t)a * dim);
           const uint4* B4 = reinterpret_cast<const uint4*>(data + (size_t)c * dim);
           auto load = [&](uint32_t u, int w) { return __ldg((w ? B4 : A4) + u); };
-          level2_pair_rounds(load, (int)sub, dim >> 3, x, y);
+          // the 960-dim width at compile time, so that the quarter's loads
+          // are issued ahead of its sums
+          if (dim == 960)
+            level2_pair_fixed<120>(load, (int)sub, x, y);
+          else
+            level2_pair_rounds(load, (int)sub, dim >> 3, x, y);
         }
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
