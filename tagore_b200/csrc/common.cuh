@@ -86,13 +86,15 @@ __device__ __forceinline__ float warp_dist(const __half* __restrict__ a, const _
 }
 
 // Four independent distances against one query, interleaving their shuffle
-// trees. Rows with id kInv yield 0 and must be ignored by the caller.
+// trees. Rows with id kInv yield 0 and must be ignored by the caller. DIM,
+// when given, fixes the width at compile time (`dim` is then DIM).
+template <uint32_t DIM = 0>
 __device__ __forceinline__ void warp_dist4(const __half* __restrict__ q, const __half* __restrict__ base,
                                            uint32_t dim, const uint32_t ids[4], float out[4],
                                            int lane) {
   float x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f};
-  const uint32_t chunks = dim >> 2;
-  for (uint32_t j = lane; j < chunks; j += 32) {
+  if constexpr (DIM != 0) dim = DIM;
+  auto chunk = [&](uint32_t j) {
     const uint2 vq = *(reinterpret_cast<const uint2*>(q) + j);
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
@@ -101,6 +103,14 @@ __device__ __forceinline__ void warp_dist4(const __half* __restrict__ q, const _
         chunk_acc(vq, vb, x[t], y[t]);
       }
     }
+  };
+  if constexpr (DIM != 0) {
+#pragma unroll
+    for (uint32_t i = 0; i < (DIM / 4 + 31) / 32; ++i)
+      if (lane + 32 * i < DIM / 4) chunk(lane + 32 * i);
+  } else {
+    const uint32_t chunks = dim >> 2;
+    for (uint32_t j = lane; j < chunks; j += 32) chunk(j);
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {

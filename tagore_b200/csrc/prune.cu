@@ -545,7 +545,8 @@ static __device__ __noinline__ uint32_t warp_filter_group(const uint32_t* cand, 
       if constexpr (G == 8)
         warp_dist8_d96(crow, data, ids, o, lane);
       else
-        warp_dist4(crow, data, dim, ids, o, lane);
+        dim == 960 ? warp_dist4<960>(crow, data, dim, ids, o, lane)
+                   : warp_dist4(crow, data, dim, ids, o, lane);
 #pragma unroll
       for (int t = 0; t < G; ++t) {
         if (ids[t] == kInv) continue;
@@ -718,7 +719,8 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
       for (uint32_t i = 0; i < kSelectCand; i += 4) {
         const uint32_t ids[4] = {cand[K + i], cand[K + i + 1], cand[K + i + 2], cand[K + i + 3]};
         float o[4];
-        warp_dist4(q, data, dim, ids, o, lane);
+        dim == 960 ? warp_dist4<960>(q, data, dim, ids, o, lane)
+                   : warp_dist4(q, data, dim, ids, o, lane);
         if (lane < 4) cdis[K + i + lane] = lane == 0 ? o[0] : lane == 1 ? o[1] : lane == 2 ? o[2] : o[3];
       }
     }
@@ -990,7 +992,10 @@ __global__ void __launch_bounds__(kDpgThreads, 1)
       float r4[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) ids[q] = (m0 + q < K) ? nei0[m0 + q] : kInv;
-      warp_dist4(data + (size_t)nei0[a] * dim, data, dim, ids, r4, lane);
+      if (dim == 960)
+        warp_dist4<960>(data + (size_t)nei0[a] * dim, data, dim, ids, r4, lane);
+      else
+        warp_dist4(data + (size_t)nei0[a] * dim, data, dim, ids, r4, lane);
       if (lane < 4 && m0 + lane < K) {
         const float r = lane == 0 ? r4[0] : lane == 1 ? r4[1] : lane == 2 ? r4[2] : r4[3];
         if (r < nrow[m0 + lane]) atomicAdd(&det[m0 + lane], 1u);
