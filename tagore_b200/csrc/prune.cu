@@ -545,8 +545,9 @@ static __device__ __noinline__ uint32_t warp_filter_group(const uint32_t* cand, 
       if constexpr (G == 8)
         warp_dist8_d96(crow, data, ids, o, lane);
       else
-        dim == 960 ? warp_dist4<960>(crow, data, dim, ids, o, lane)
-                   : warp_dist4(crow, data, dim, ids, o, lane);
+        dim == 960   ? warp_dist4<960>(crow, data, dim, ids, o, lane)
+        : dim == 128 ? warp_dist4<128>(crow, data, dim, ids, o, lane)
+                     : warp_dist4(crow, data, dim, ids, o, lane);
 #pragma unroll
       for (int t = 0; t < G; ++t) {
         if (ids[t] == kInv) continue;
