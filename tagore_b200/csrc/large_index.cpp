@@ -102,6 +102,39 @@ void cluster_order(const std::vector<uint32_t>& inter, uint32_t C, uint32_t bs,
   }
 }
 
+// Membership of the up to 2K ids of two rows without an N-sized array: open
+// addressing over at least 4K slots (load <= 1/2), cleared in O(1) by a
+// generation tag.
+struct IdSet {
+  std::vector<uint32_t> key, tag;
+  uint32_t mask = 0, shift = 0, gen = 0;
+  explicit IdSet(uint32_t K) {
+    uint32_t bits = 6;
+    while ((1u << bits) < 4u * K) ++bits;
+    key.assign(1u << bits, 0);
+    tag.assign(1u << bits, 0);
+    mask = (1u << bits) - 1u;
+    shift = 32 - bits;
+  }
+  void clear() {
+    if (++gen == 0) {  // the tags wrapped: reset them once
+      std::fill(tag.begin(), tag.end(), 0u);
+      gen = 1;
+    }
+  }
+  // Inserts id; false if it was already there.
+  bool insert(uint32_t id) {
+    uint32_t h = (id * 0x9E3779B1u) >> shift;
+    while (tag[h] == gen) {
+      if (key[h] == id) return false;
+      h = (h + 1) & mask;
+    }
+    tag[h] = gen;
+    key[h] = id;
+    return true;
+  }
+};
+
 struct Built {
   LocalRows rows;  // n x K, [deg, global ids...]
   uint32_t medoid = 0;
@@ -271,7 +304,7 @@ int merge_all(const TagoreLargeParams& p, const std::vector<std::vector<uint32_t
   std::vector<std::string> part_msg(R);  // the library's error text is per thread
   auto final_part = [&](uint32_t r) {
     std::vector<Reader> shard(C);
-    std::vector<uint8_t> mark(N, 0);
+    IdSet seen(K);
     std::vector<uint32_t> a(K), b(K), nh;
     std::vector<uint32_t>& o = part_out[r];
     auto reader = [&](uint32_t c) -> Reader* {
@@ -311,16 +344,13 @@ int merge_all(const TagoreLargeParams& p, const std::vector<std::vector<uint32_t
              d2 <= K && f2->get(b.data(), 4ull * d2);
         if (ok) {
           nh.clear();
-          for (uint32_t j = 0; j < d1; ++j) {
-            mark[a[j]] = 1;
+          seen.clear();
+          for (uint32_t j = 0; j < d1; ++j) {  // the first row whole, as the reference
+            seen.insert(a[j]);
             nh.push_back(a[j]);
           }
           for (uint32_t j = 0; j < d2; ++j)
-            if (!mark[b[j]]) {
-              mark[b[j]] = 1;
-              nh.push_back(b[j]);
-            }
-          for (uint32_t v : nh) mark[v] = 0;
+            if (seen.insert(b[j])) nh.push_back(b[j]);
           const uint32_t deg = std::min<uint32_t>((uint32_t)nh.size(), maxd);
           o.push_back(deg);
           o.insert(o.end(), nh.begin(), nh.begin() + deg);
