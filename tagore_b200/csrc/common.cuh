@@ -85,6 +85,52 @@ __device__ __forceinline__ float warp_dist(const __half* __restrict__ a, const _
   return warp_tree(x, y);
 }
 
+// A query row's chunks as one lane holds them in the reference's lane order
+// (chunk lane + 32 i in v[i]), for a width DIM fixed at compile time: loaded
+// once, reused by every distance against that query.
+template <uint32_t DIM>
+struct QRow {
+  static constexpr uint32_t kChunks = DIM / 4, kPerLane = (kChunks + 31) / 32;
+  uint2 v[kPerLane];
+};
+
+template <uint32_t DIM>
+__device__ __forceinline__ void load_qrow(const __half* __restrict__ q, QRow<DIM>& r, int lane) {
+#pragma unroll
+  for (uint32_t i = 0; i < QRow<DIM>::kPerLane; ++i) {
+    const uint32_t j = lane + 32 * i;
+    r.v[i] = j < QRow<DIM>::kChunks ? *(reinterpret_cast<const uint2*>(q) + j) : make_uint2(0u, 0u);
+  }
+}
+
+// warp_dist4 against a preloaded query row.
+template <uint32_t DIM>
+__device__ __forceinline__ void warp_dist4_q(const QRow<DIM>& qr, const __half* __restrict__ base,
+                                             const uint32_t ids[4], float out[4], int lane) {
+  float x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (uint32_t i = 0; i < QRow<DIM>::kPerLane; ++i) {
+    const uint32_t j = lane + 32 * i;
+    if (j < QRow<DIM>::kChunks) {
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        if (ids[t] != kInv) {
+          const uint2 vb = __ldg(reinterpret_cast<const uint2*>(base + (size_t)ids[t] * DIM) + j);
+          chunk_acc(qr.v[i], vb, x[t], y[t]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+      add2(x[t], y[t], __shfl_down_sync(kFull, x[t], off), __shfl_down_sync(kFull, y[t], off));
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) out[t] = __shfl_sync(kFull, __fadd_rn(x[t], y[t]), 0);
+}
+
 // Four independent distances against one query, interleaving their shuffle
 // trees. Rows with id kInv yield 0 and must be ignored by the caller. DIM,
 // when given, fixes the width at compile time (`dim` is then DIM).

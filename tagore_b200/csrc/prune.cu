@@ -518,8 +518,11 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
 // candidate is dropped when any of its tests fires, whichever fires first,
 // so the kept set and the return value are those of warp_filter.
 // G kept neighbours per step: 8 at 96 dims (warp_dist8_d96, a half-warp per
-// distance), 4 otherwise (warp_dist4).
-template <int G>
+// distance), 4 otherwise (warp_dist4). DIM != 0 fixes the width at compile
+// time. At 128 dims (one chunk per lane) the candidate's chunk is loaded once
+// for all its tests; at 960 the eight chunks a lane would hold cost more in
+// registers than their reloads (NSSG at 1M x 960: 0.80 s against 0.54 s).
+template <int G, uint32_t DIM>
 static __device__ __noinline__ uint32_t warp_filter_group(const uint32_t* cand, const float* cdis,
                                                           uint32_t len, uint32_t bid, uint32_t fd,
                                                           int metric, float thre,
@@ -533,6 +536,10 @@ static __device__ __noinline__ uint32_t warp_filter_group(const uint32_t* cand, 
     const float dc = cdis[i];
     const __half* crow = data + (size_t)c * dim;
     bool keep = true;
+    constexpr bool kPreload = G == 4 && DIM != 0 && DIM <= 128;
+    [[maybe_unused]] QRow<kPreload ? DIM : 4u> qr;
+    if constexpr (kPreload)
+      if (nsel > 0) load_qrow(crow, qr, lane);
     for (uint32_t s0 = 0; s0 < nsel && keep; s0 += G) {
       uint32_t ids[G];
       float o[G];
@@ -544,10 +551,10 @@ static __device__ __noinline__ uint32_t warp_filter_group(const uint32_t* cand, 
       if (!keep) break;
       if constexpr (G == 8)
         warp_dist8_d96(crow, data, ids, o, lane);
+      else if constexpr (kPreload)
+        warp_dist4_q<DIM>(qr, data, ids, o, lane);
       else
-        dim == 960   ? warp_dist4<960>(crow, data, dim, ids, o, lane)
-        : dim == 128 ? warp_dist4<128>(crow, data, dim, ids, o, lane)
-                     : warp_dist4(crow, data, dim, ids, o, lane);
+        warp_dist4<DIM>(crow, data, dim, ids, o, lane);
 #pragma unroll
       for (int t = 0; t < G; ++t) {
         if (ids[t] == kInv) continue;
@@ -589,10 +596,17 @@ static __device__ __forceinline__ uint32_t warp_filter_wide(const uint32_t* cand
                                                             const __half* __restrict__ data,
                                                             uint32_t dim, uint32_t* sel, float* seld,
                                                             int lane, uint32_t* scored) {
-  return dim == 96 ? warp_filter_group<8>(cand, cdis, len, bid, fd, metric, thre, data, dim, sel,
-                                          seld, lane, scored)
-                   : warp_filter_group<4>(cand, cdis, len, bid, fd, metric, thre, data, dim, sel,
-                                          seld, lane, scored);
+  if (dim == 96)
+    return warp_filter_group<8, 96>(cand, cdis, len, bid, fd, metric, thre, data, dim, sel, seld,
+                                    lane, scored);
+  if (dim == 960)
+    return warp_filter_group<4, 960>(cand, cdis, len, bid, fd, metric, thre, data, dim, sel, seld,
+                                     lane, scored);
+  if (dim == 128)
+    return warp_filter_group<4, 128>(cand, cdis, len, bid, fd, metric, thre, data, dim, sel, seld,
+                                     lane, scored);
+  return warp_filter_group<4, 0>(cand, cdis, len, bid, fd, metric, thre, data, dim, sel, seld,
+                                 lane, scored);
 }
 
 // Per-warp shared layout of the select kernels: the beam (path collect) and
@@ -717,12 +731,19 @@ __global__ void __launch_bounds__(kWarps * 32, 6)
       // lane reads its 8-byte chunks of four rows at once (coalesced across
       // the warp) and the four shuffle trees interleave. Same lane order as
       // the thread-serial distance, so the same values.
-      for (uint32_t i = 0; i < kSelectCand; i += 4) {
-        const uint32_t ids[4] = {cand[K + i], cand[K + i + 1], cand[K + i + 2], cand[K + i + 3]};
-        float o[4];
-        dim == 960 ? warp_dist4<960>(q, data, dim, ids, o, lane)
-                   : warp_dist4(q, data, dim, ids, o, lane);
-        if (lane < 4) cdis[K + i + lane] = lane == 0 ? o[0] : lane == 1 ? o[1] : lane == 2 ? o[2] : o[3];
+      auto score = [&](auto&& dist4) {
+        for (uint32_t i = 0; i < kSelectCand; i += 4) {
+          const uint32_t ids[4] = {cand[K + i], cand[K + i + 1], cand[K + i + 2], cand[K + i + 3]};
+          float o[4];
+          dist4(ids, o);
+          if (lane < 4)
+            cdis[K + i + lane] = lane == 0 ? o[0] : lane == 1 ? o[1] : lane == 2 ? o[2] : o[3];
+        }
+      };
+      if (dim == 960) {
+        score([&](const uint32_t* ids, float* o) { warp_dist4<960>(q, data, dim, ids, o, lane); });
+      } else {
+        score([&](const uint32_t* ids, float* o) { warp_dist4(q, data, dim, ids, o, lane); });
       }
     }
     for (uint32_t i = lane; i < K; i += 32) {
