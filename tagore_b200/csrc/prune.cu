@@ -510,14 +510,13 @@ __device__ uint32_t warp_filter(const uint32_t* cand, const float* cdis, uint32_
   return nsel;
 }
 
-// The same filter for rows wider than 128 halves, warp-cooperative. A
-// thread-serial distance over such rows is a long chain of scattered 16-byte
+// The same filter, warp-cooperative (where wide_filter picks it). A
+// thread-serial distance over a wide row is a long chain of scattered 16-byte
 // loads per lane; here the warp takes the candidates in list order and tests
-// each against the kept neighbours four at a time with coalesced row reads
-// (warp_dist4), stopping at the first group in which a rule fires. A
-// candidate is dropped when any of its tests fires, whichever fires first,
-// so the kept set and the return value are those of warp_filter.
-// G kept neighbours per step: 8 at 96 dims (warp_dist8_d96, a half-warp per
+// each against the kept neighbours G at a time with coalesced row reads,
+// stopping at the first group in which a rule fires. A candidate is dropped
+// when any of its tests fires, whichever fires first, so the kept set and the
+// return value are those of warp_filter. G kept neighbours per step: 8 at 96 dims (warp_dist8_d96, a half-warp per
 // distance), 4 otherwise (warp_dist4). DIM != 0 fixes the width at compile
 // time. At 128 dims (one chunk per lane) the candidate's chunk is loaded once
 // for all its tests; at 960 the eight chunks a lane would hold cost more in
@@ -581,11 +580,11 @@ static __device__ __noinline__ uint32_t warp_filter_group(const uint32_t* cand, 
 
 // Which filter a prune runs. Measured at 1M-2M nodes: the cooperative filter
 // wins wherever the thread-serial tree is not the 128-dim one (d = 96: the
-// Vamana select 1,098 -> 559 ms; d = 960: NSSG 5.5 -> 0.73 s) and, at 128
+// Vamana select 1,098 -> 466 ms; d = 960: NSSG 5.5 -> 0.51 s) and, at 128
 // dims, where alpha > 1 keeps long lists that take many tests per candidate
-// (Vamana 1.2: 262 -> 183 ms). At 128 dims with alpha 1 most candidates fall
+// (Vamana 1.2: 262 -> 170 ms). At 128 dims with alpha 1 most candidates fall
 // to their first tests, and 32 lanes each working through its own candidate
-// keep more loads in flight (NSG select 203 ms against 254).
+// keep more loads in flight (NSG select 203 ms against 226).
 __device__ __forceinline__ bool wide_filter(uint32_t dim, int metric, float thre) {
   return dim != 128 || (metric == 0 && thre > 1.0f);
 }
